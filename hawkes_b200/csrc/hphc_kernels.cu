@@ -1,0 +1,602 @@
+// Pair-sum kernels of the B200 Hawkes likelihood engine.
+//
+// The reference evaluates, for every target event i, the rate
+//   lambda_i = sum_j B_ij + S_ij   (src/NewHawkes.hpp:520-547)
+// with one work-group of 128 threads per event striding over j
+// (src/backend/opencl/OpenCLHawkes.hpp:632-702).  Here a CTA owns a strip of
+// kSweepThreads * R target events (R per thread, in registers) and a range of
+// j tiles; each kTile-event j tile is staged in shared memory with coalesced
+// 16-byte loads and read back as broadcasts.  Per (strip, tile) the CTA
+// decides from FP64 time bounds whether the tile pair has any background term
+// above the underflow threshold, any causal (t_j < t_i) self-excitation term,
+// and whether the causal mask is needed, so the non-causal half of the
+// self-excitation sum is skipped at tile level.  Skipped terms are exactly zero
+// in the working precision, so skipping does not change any bit of the result.
+//
+// All sums are written per (chunk, event) and combined in chunk order, then
+// reduced over events with fixed shuffle trees: results do not depend on
+// scheduling.
+#include <math.h>
+
+#include "hphc_kernels.cuh"
+
+namespace hphc {
+namespace {
+
+constexpr double kInvSqrt2Pi = 0.398942280401432677939946059934;
+constexpr double kSqrtHalf = 0.707106781186547524400844362105;
+constexpr int kFlush = 32;  // FP32 partial sums are moved into FP64 every kFlush j events
+
+__device__ __forceinline__ float ex2_ftz(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// ---------------------------------------------------------------- packing --
+
+template <int D>
+__global__ void pack_f64_kernel(int N, const double* __restrict__ loc,
+                                const double* __restrict__ times, double* __restrict__ rec) {
+    constexpr int S = Layout<D>::kF64Stride;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    double* r = rec + (size_t)i * S;
+#pragma unroll
+    for (int k = 0; k < D; ++k) r[k] = loc[(size_t)i * D + k];
+    r[D] = times[i];
+#pragma unroll
+    for (int k = D + 1; k < S; ++k) r[k] = 0.0;
+}
+
+template <int D>
+__global__ void pack_f32_kernel(int N, const double* __restrict__ loc,
+                                const double* __restrict__ times, const int32_t* __restrict__ ranks,
+                                float* __restrict__ rec) {
+    constexpr int S = Layout<D>::kF32Stride;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    float* r = rec + (size_t)i * S;
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        const double v = loc[(size_t)i * D + k];
+        const float h = (float)v;
+        r[k] = h;
+        r[D + 1 + k] = (float)(v - (double)h);
+    }
+    const double v = times[i];
+    const float h = (float)v;
+    r[D] = h;
+    r[2 * D + 1] = (float)(v - (double)h);
+    r[2 * D + 2] = __int_as_float(ranks[i]);
+#pragma unroll
+    for (int k = 2 * D + 3; k < S; ++k) r[k] = 0.0f;
+}
+
+// One CTA of kTile threads per tile: min and max of t over the tile.
+__global__ void __launch_bounds__(kTile)
+tile_bounds_kernel(int N, const double* __restrict__ times, double* __restrict__ tileMin,
+                   double* __restrict__ tileMax) {
+    __shared__ double sMin[kTile / 32], sMax[kTile / 32];
+    const int j = blockIdx.x * kTile + threadIdx.x;
+    double lo = INFINITY, hi = -INFINITY;
+    if (j < N) lo = hi = times[j];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = fmin(lo, __shfl_down_sync(0xffffffffu, lo, o));
+        hi = fmax(hi, __shfl_down_sync(0xffffffffu, hi, o));
+    }
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        sMin[w] = lo;
+        sMax[w] = hi;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 1; k < kTile / 32; ++k) {
+            lo = fmin(lo, sMin[k]);
+            hi = fmax(hi, sMax[k]);
+        }
+        tileMin[blockIdx.x] = lo;
+        tileMax[blockIdx.x] = hi;
+    }
+}
+
+// ------------------------------------------------------ tile-pair decision --
+
+struct TileMode {
+    bool doB, doS, allCausal;
+};
+
+// dt = t_i - t_j over the tile pair lies in [tminI - tmaxJ, tmaxI - tminJ].
+__device__ __forceinline__ TileMode tile_mode(double tminI, double tmaxI, double tminJ,
+                                              double tmaxJ, const PairConsts& c) {
+    const double dtLo = tminI - tmaxJ, dtHi = tmaxI - tminJ;
+    const double minAbs = dtLo > 0.0 ? dtLo : (dtHi < 0.0 ? -dtHi : 0.0);
+    TileMode m;
+    m.doB = !(c.skipB >= 0.0 && -c.cB * minAbs * minAbs >= c.skipB);
+    m.allCausal = dtLo > 0.0;
+    const bool anyCausal = dtHi > 0.0;
+    m.doS = anyCausal && !(c.skipS >= 0.0 && m.allCausal && -c.cW * dtLo >= c.skipS);
+    return m;
+}
+
+// ----------------------------------------------------------- FP64 sweep --
+
+template <int D, int R, bool DO_B, bool DO_S, bool MASK>
+__device__ __forceinline__ void body_f64(const double* __restrict__ sRec, int nj,
+                                         const double (&xi)[R][D], const double (&ti)[R],
+                                         const PairConsts& c, double (&acc)[R][kNumAcc]) {
+    constexpr int S = Layout<D>::kF64Stride;
+#pragma unroll 2
+    for (int j = 0; j < nj; ++j) {
+        double rj[S];
+#pragma unroll
+        for (int v = 0; v < S / 2; ++v) {
+            const double2 q = reinterpret_cast<const double2*>(sRec + j * S)[v];
+            rj[2 * v] = q.x;
+            rj[2 * v + 1] = q.y;
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            double d2 = 0.0;
+#pragma unroll
+            for (int k = 0; k < D; ++k) {
+                const double dd = xi[r][k] - rj[k];
+                d2 = fma(dd, dd, d2);
+            }
+            const double dt = ti[r] - rj[D];
+            if (DO_B) {
+                const double t2 = dt * dt;
+                const double B = exp(fma(c.cA, d2, c.cB * t2));
+                acc[r][0] += B;
+                acc[r][1] = fma(B, d2, acc[r][1]);
+                acc[r][2] = fma(B, t2, acc[r][2]);
+            }
+            if (DO_S) {
+                double Sv = exp(fma(c.cS, d2, c.cW * dt));
+                if (MASK) Sv = dt > 0.0 ? Sv : 0.0;
+                acc[r][3] += Sv;
+                acc[r][4] = fma(Sv, d2, acc[r][4]);
+                acc[r][5] = fma(Sv, dt, acc[r][5]);
+            }
+        }
+    }
+}
+
+template <int D, int R>
+__global__ void __launch_bounds__(kSweepThreads)
+sweep_f64_kernel(SweepGeometry g, const double* __restrict__ rec,
+                 const double* __restrict__ tileMin, const double* __restrict__ tileMax,
+                 PairConsts c, double* __restrict__ partials) {
+    constexpr int S = Layout<D>::kF64Stride;
+    __shared__ __align__(16) double sRec[kTile * S];
+    const int tid = threadIdx.x;
+    const int strip = blockIdx.x / g.nChunks;
+    const int chunk = blockIdx.x - strip * g.nChunks;
+    const int stripBase = strip * kSweepThreads * R;
+
+    double xi[R][D], ti[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int i = min(stripBase + r * kSweepThreads + tid, g.N - 1);
+#pragma unroll
+        for (int k = 0; k < D; ++k) xi[r][k] = rec[(size_t)i * S + k];
+        ti[r] = rec[(size_t)i * S + D];
+    }
+    double tminI = INFINITY, tmaxI = -INFINITY;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int tt = stripBase / kTile + r;
+        if (tt < g.nTiles) {
+            tminI = fmin(tminI, tileMin[tt]);
+            tmaxI = fmax(tmaxI, tileMax[tt]);
+        }
+    }
+    double acc[R][kNumAcc];
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+        for (int q = 0; q < kNumAcc; ++q) acc[r][q] = 0.0;
+
+    const int jt0 = chunk * g.chunkTiles;
+    const int jt1 = min(jt0 + g.chunkTiles, g.nTiles);
+    for (int jt = jt0; jt < jt1; ++jt) {
+        const TileMode m = tile_mode(tminI, tmaxI, tileMin[jt], tileMax[jt], c);
+        if (!m.doB && !m.doS) continue;
+        const int j0 = jt * kTile;
+        const int nj = min(kTile, g.N - j0);
+        __syncthreads();
+        const double2* src = reinterpret_cast<const double2*>(rec + (size_t)j0 * S);
+        double2* dst = reinterpret_cast<double2*>(sRec);
+        for (int v = tid; v < nj * (S / 2); v += kSweepThreads) dst[v] = src[v];
+        __syncthreads();
+        if (m.doB) {
+            if (!m.doS)
+                body_f64<D, R, true, false, false>(sRec, nj, xi, ti, c, acc);
+            else if (m.allCausal)
+                body_f64<D, R, true, true, false>(sRec, nj, xi, ti, c, acc);
+            else
+                body_f64<D, R, true, true, true>(sRec, nj, xi, ti, c, acc);
+        } else {
+            if (m.allCausal)
+                body_f64<D, R, false, true, false>(sRec, nj, xi, ti, c, acc);
+            else
+                body_f64<D, R, false, true, true>(sRec, nj, xi, ti, c, acc);
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int i = stripBase + r * kSweepThreads + tid;
+        if (i < g.N) {
+#pragma unroll
+            for (int q = 0; q < kNumAcc; ++q)
+                partials[((size_t)chunk * kNumAcc + q) * g.Npad + i] = acc[r][q];
+        }
+    }
+}
+
+// ------------------------------------------------ FP32-compensated sweep --
+//
+// Differences are formed from hi/lo float pairs, dd = (hi_i - hi_j) + (lo_i - lo_j),
+// so the FP32 representation error of the inputs (ulp(8760 h) ~ 1e-3 h) never
+// enters dt or d.  The exponent coefficients are split hi + lo as well, so
+// their FP32 rounding does not bias every term in the same direction.  The
+// six sums are kept in FP32 over kFlush consecutive j and then added to FP64
+// accumulators (blocked compensated summation); the cross-tile, cross-chunk
+// and per-event finish are FP64.
+
+template <int D, int R, bool DO_B, bool DO_S, bool MASK>
+__device__ __forceinline__ void body_f32(const float* __restrict__ sRec, int jb, int je,
+                                         const float (&xh)[R][D], const float (&xl)[R][D],
+                                         const float (&th)[R], const float (&tl)[R],
+                                         const int (&rk)[R], const PairConsts& c,
+                                         float (&a)[R][kNumAcc]) {
+    constexpr int S = Layout<D>::kF32Stride;
+#pragma unroll 4
+    for (int j = jb; j < je; ++j) {
+        float rj[S];
+#pragma unroll
+        for (int v = 0; v < S / 4; ++v) {
+            const float4 q = reinterpret_cast<const float4*>(sRec + j * S)[v];
+            rj[4 * v] = q.x;
+            rj[4 * v + 1] = q.y;
+            rj[4 * v + 2] = q.z;
+            rj[4 * v + 3] = q.w;
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            float d2 = 0.0f;
+#pragma unroll
+            for (int k = 0; k < D; ++k) {
+                const float dd = (xh[r][k] - rj[k]) + (xl[r][k] - rj[D + 1 + k]);
+                d2 = fmaf(dd, dd, d2);
+            }
+            const float dt = (th[r] - rj[D]) + (tl[r] - rj[2 * D + 1]);
+            if (DO_B) {
+                const float t2 = dt * dt;
+                const float e =
+                    fmaf(c.fAh, d2, fmaf(c.fBh, t2, fmaf(c.fAl, d2, fmaf(c.fBl, t2, c.ex2Fix))));
+                const float B = ex2_ftz(e);
+                a[r][0] += B;
+                a[r][1] = fmaf(B, d2, a[r][1]);
+                a[r][2] = fmaf(B, t2, a[r][2]);
+            }
+            if (DO_S) {
+                const float e =
+                    fmaf(c.fSh, d2, fmaf(c.fWh, dt, fmaf(c.fSl, d2, fmaf(c.fWl, dt, c.ex2Fix))));
+                float Sv = ex2_ftz(e);
+                if (MASK) Sv = rk[r] > __float_as_int(rj[2 * D + 2]) ? Sv : 0.0f;
+                a[r][3] += Sv;
+                a[r][4] = fmaf(Sv, d2, a[r][4]);
+                a[r][5] = fmaf(Sv, dt, a[r][5]);
+            }
+        }
+    }
+}
+
+template <int D, int R, bool DO_B, bool DO_S, bool MASK>
+__device__ __forceinline__ void tile_f32(const float* __restrict__ sRec, int nj,
+                                         const float (&xh)[R][D], const float (&xl)[R][D],
+                                         const float (&th)[R], const float (&tl)[R],
+                                         const int (&rk)[R], const PairConsts& c,
+                                         double (&acc)[R][kNumAcc]) {
+    for (int jb = 0; jb < nj; jb += kFlush) {
+        float a[R][kNumAcc];
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+#pragma unroll
+            for (int q = 0; q < kNumAcc; ++q) a[r][q] = 0.0f;
+        body_f32<D, R, DO_B, DO_S, MASK>(sRec, jb, min(jb + kFlush, nj), xh, xl, th, tl, rk, c, a);
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+#pragma unroll
+            for (int q = 0; q < kNumAcc; ++q) acc[r][q] += (double)a[r][q];
+    }
+}
+
+template <int D, int R>
+__global__ void __launch_bounds__(kSweepThreads)
+sweep_f32c_kernel(SweepGeometry g, const float* __restrict__ rec,
+                  const double* __restrict__ tileMin, const double* __restrict__ tileMax,
+                  PairConsts c, double* __restrict__ partials) {
+    constexpr int S = Layout<D>::kF32Stride;
+    __shared__ __align__(16) float sRec[kTile * S];
+    const int tid = threadIdx.x;
+    const int strip = blockIdx.x / g.nChunks;
+    const int chunk = blockIdx.x - strip * g.nChunks;
+    const int stripBase = strip * kSweepThreads * R;
+
+    float xh[R][D], xl[R][D], th[R], tl[R];
+    int rk[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int i = min(stripBase + r * kSweepThreads + tid, g.N - 1);
+        const float* ri = rec + (size_t)i * S;
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+            xh[r][k] = ri[k];
+            xl[r][k] = ri[D + 1 + k];
+        }
+        th[r] = ri[D];
+        tl[r] = ri[2 * D + 1];
+        rk[r] = __float_as_int(ri[2 * D + 2]);
+    }
+    double tminI = INFINITY, tmaxI = -INFINITY;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int tt = stripBase / kTile + r;
+        if (tt < g.nTiles) {
+            tminI = fmin(tminI, tileMin[tt]);
+            tmaxI = fmax(tmaxI, tileMax[tt]);
+        }
+    }
+    double acc[R][kNumAcc];
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+        for (int q = 0; q < kNumAcc; ++q) acc[r][q] = 0.0;
+
+    const int jt0 = chunk * g.chunkTiles;
+    const int jt1 = min(jt0 + g.chunkTiles, g.nTiles);
+    for (int jt = jt0; jt < jt1; ++jt) {
+        const TileMode m = tile_mode(tminI, tmaxI, tileMin[jt], tileMax[jt], c);
+        if (!m.doB && !m.doS) continue;
+        const int j0 = jt * kTile;
+        const int nj = min(kTile, g.N - j0);
+        __syncthreads();
+        const float4* src = reinterpret_cast<const float4*>(rec + (size_t)j0 * S);
+        float4* dst = reinterpret_cast<float4*>(sRec);
+        for (int v = tid; v < nj * (S / 4); v += kSweepThreads) dst[v] = src[v];
+        __syncthreads();
+        if (m.doB) {
+            if (!m.doS)
+                tile_f32<D, R, true, false, false>(sRec, nj, xh, xl, th, tl, rk, c, acc);
+            else if (m.allCausal)
+                tile_f32<D, R, true, true, false>(sRec, nj, xh, xl, th, tl, rk, c, acc);
+            else
+                tile_f32<D, R, true, true, true>(sRec, nj, xh, xl, th, tl, rk, c, acc);
+        } else {
+            if (m.allCausal)
+                tile_f32<D, R, false, true, false>(sRec, nj, xh, xl, th, tl, rk, c, acc);
+            else
+                tile_f32<D, R, false, true, true>(sRec, nj, xh, xl, th, tl, rk, c, acc);
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const int i = stripBase + r * kSweepThreads + tid;
+        if (i < g.N) {
+#pragma unroll
+            for (int q = 0; q < kNumAcc; ++q)
+                partials[((size_t)chunk * kNumAcc + q) * g.Npad + i] = acc[r][q];
+        }
+    }
+}
+
+// ------------------------------------------------------------- finish --
+
+// Deterministic CTA sum of NV values per thread; result valid in thread 0.
+template <int NV, int THREADS>
+__device__ __forceinline__ void block_sum(double (&v)[NV]) {
+    __shared__ double sWarp[THREADS / 32][NV];
+#pragma unroll
+    for (int q = 0; q < NV; ++q)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0)
+#pragma unroll
+        for (int q = 0; q < NV; ++q) sWarp[w][q] = v[q];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < NV; ++q) {
+            double s = sWarp[0][q];
+            for (int k = 1; k < THREADS / 32; ++k) s += sWarp[k][q];
+            v[q] = s;
+        }
+    }
+}
+
+__device__ __forceinline__ double std_normal_cdf(double v) { return 0.5 * erfc(-v * kSqrtHalf); }
+
+__global__ void __launch_bounds__(kFinishThreads)
+finish_kernel(SweepGeometry g, const double* __restrict__ partials,
+              const double* __restrict__ times, FinishConsts f, double* __restrict__ blockSums,
+              double* __restrict__ probs) {
+    const int i = blockIdx.x * kFinishThreads + threadIdx.x;
+    double v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = 0.0;
+    if (i < g.N) {
+        double s[kNumAcc];
+#pragma unroll
+        for (int q = 0; q < kNumAcc; ++q) {
+            double acc = 0.0;
+            for (int ch = 0; ch < g.nChunks; ++ch)
+                acc += partials[((size_t)ch * kNumAcc + q) * g.Npad + i];
+            s[q] = acc;
+        }
+        const double SB = f.prefB * s[0];
+        const double SS = f.prefS * s[3];
+        const double lam = SB + SS;
+        const double inv = 1.0 / lam;
+        const double ti = times[i];
+        const double Di = f.T - ti;
+        const double eW = exp(-f.omega * Di);
+        const double cdf = std_normal_cdf(f.b * Di) - std_normal_cdf(-f.b * ti);
+        v[0] = log(lam) + f.theta * (eW - 1.0) - f.mu0 * cdf;
+        v[1] = ((double)f.D / f.sigma * SS - f.sigma * f.prefS * s[4]) * inv;
+        v[2] = ((double)f.D / f.a * SB - f.a * f.prefB * s[1]) * inv;
+        const double bD = f.b * Di, bt = f.b * ti;
+        const double phiD = kInvSqrt2Pi * exp(-0.5 * bD * bD);
+        const double phiT = kInvSqrt2Pi * exp(-0.5 * bt * bt);
+        v[3] = (SB / f.b - f.b * f.prefB * s[2]) * inv - f.mu0 * (phiD * Di + phiT * ti);
+        v[4] = (SS / f.omega - f.prefS * s[5]) * inv - f.theta * Di * eW;
+        v[5] = f.seScale * s[3] * inv + (eW - 1.0);
+        v[6] = f.bgScale * s[0] * inv - cdf;
+        if (probs) probs[i] = SS * inv;
+    }
+    block_sum<8, kFinishThreads>(v);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) blockSums[(size_t)blockIdx.x * 8 + q] = v[q];
+    }
+}
+
+// Mean relative error of ex2.approx.ftz.f32 against FP64 exp2 over arguments
+// spread uniformly on [-16, 0) (uniform fractional parts): per-CTA sums of
+// ex2(x) / 2^x - 1, added by the host in CTA order.
+__global__ void __launch_bounds__(kFinishThreads)
+ex2_bias_kernel(int n, double* __restrict__ blockSums) {
+    const int i = blockIdx.x * kFinishThreads + threadIdx.x;
+    double v[1] = {0.0};
+    if (i < n) {
+        const float x = (float)(-16.0 * ((double)i + 0.5) / (double)n);
+        v[0] = (double)ex2_ftz(x) / exp2((double)x) - 1.0;
+    }
+    block_sum<1, kFinishThreads>(v);
+    if (threadIdx.x == 0) blockSums[blockIdx.x] = v[0];
+}
+
+constexpr int kFinalThreads = 256;
+
+__global__ void __launch_bounds__(kFinalThreads)
+final_kernel(int nBlocks, const double* __restrict__ blockSums, FinishConsts f,
+             double* __restrict__ out) {
+    double v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = 0.0;
+    for (int b = threadIdx.x; b < nBlocks; b += kFinalThreads)
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v[q] += blockSums[(size_t)b * 8 + q];
+    block_sum<8, kFinalThreads>(v);
+    if (threadIdx.x == 0) {
+        out[0] = v[0] + f.constant;
+#pragma unroll
+        for (int q = 1; q < 7; ++q) out[q] = v[q];
+        out[7] = 0.0;
+    }
+}
+
+}  // namespace
+
+#define HPHC_FOR_EACH_DIM(X) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8)
+
+cudaError_t launch_pack_f64(int D, int N, const double* loc, const double* times, double* rec,
+                            double* tileMin, double* tileMax, cudaStream_t s) {
+    const int blocks = (N + 255) / 256;
+    switch (D) {
+#define X(d) \
+    case d: pack_f64_kernel<d><<<blocks, 256, 0, s>>>(N, loc, times, rec); break;
+        HPHC_FOR_EACH_DIM(X)
+#undef X
+        default: return cudaErrorInvalidValue;
+    }
+    tile_bounds_kernel<<<(N + kTile - 1) / kTile, kTile, 0, s>>>(N, times, tileMin, tileMax);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pack_f32(int D, int N, const double* loc, const double* times,
+                            const int32_t* ranks, float* rec, double* tileMin, double* tileMax,
+                            cudaStream_t s) {
+    const int blocks = (N + 255) / 256;
+    switch (D) {
+#define X(d) \
+    case d: pack_f32_kernel<d><<<blocks, 256, 0, s>>>(N, loc, times, ranks, rec); break;
+        HPHC_FOR_EACH_DIM(X)
+#undef X
+        default: return cudaErrorInvalidValue;
+    }
+    tile_bounds_kernel<<<(N + kTile - 1) / kTile, kTile, 0, s>>>(N, times, tileMin, tileMax);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sweep_f64(int D, int R, const SweepGeometry& g, const double* rec,
+                             const double* tileMin, const double* tileMax, const PairConsts& c,
+                             double* partials, cudaStream_t s) {
+    const int grid = g.nStrips * g.nChunks;
+#define X(d)                                                                                     \
+    case d:                                                                                      \
+        if (R == 1)                                                                              \
+            sweep_f64_kernel<d, 1><<<grid, kSweepThreads, 0, s>>>(g, rec, tileMin, tileMax, c,   \
+                                                                   partials);                    \
+        else if (R == 2)                                                                         \
+            sweep_f64_kernel<d, 2><<<grid, kSweepThreads, 0, s>>>(g, rec, tileMin, tileMax, c,   \
+                                                                   partials);                    \
+        else                                                                                     \
+            return cudaErrorInvalidValue;                                                        \
+        break;
+    switch (D) {
+        HPHC_FOR_EACH_DIM(X)
+        default: return cudaErrorInvalidValue;
+    }
+#undef X
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sweep_f32c(int D, int R, const SweepGeometry& g, const float* rec,
+                              const double* tileMin, const double* tileMax, const PairConsts& c,
+                              double* partials, cudaStream_t s) {
+    const int grid = g.nStrips * g.nChunks;
+#define X(d)                                                                                     \
+    case d:                                                                                      \
+        if (R == 2)                                                                              \
+            sweep_f32c_kernel<d, 2><<<grid, kSweepThreads, 0, s>>>(g, rec, tileMin, tileMax, c,  \
+                                                                    partials);                   \
+        else if (R == 4)                                                                         \
+            sweep_f32c_kernel<d, 4><<<grid, kSweepThreads, 0, s>>>(g, rec, tileMin, tileMax, c,  \
+                                                                    partials);                   \
+        else                                                                                     \
+            return cudaErrorInvalidValue;                                                        \
+        break;
+    switch (D) {
+        HPHC_FOR_EACH_DIM(X)
+        default: return cudaErrorInvalidValue;
+    }
+#undef X
+    return cudaGetLastError();
+}
+
+cudaError_t launch_finish(const SweepGeometry& g, const double* partials, const double* times,
+                          const FinishConsts& f, double* blockSums, double* probs,
+                          cudaStream_t s) {
+    finish_kernel<<<finish_blocks(g.N), kFinishThreads, 0, s>>>(g, partials, times, f, blockSums,
+                                                                probs);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ex2_bias(int n, double* blockSums, cudaStream_t s) {
+    ex2_bias_kernel<<<(n + kFinishThreads - 1) / kFinishThreads, kFinishThreads, 0, s>>>(
+        n, blockSums);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_final(int nBlocks, const double* blockSums, const FinishConsts& f, double* out,
+                         cudaStream_t s) {
+    final_kernel<<<1, kFinalThreads, 0, s>>>(nBlocks, blockSums, f, out);
+    return cudaGetLastError();
+}
+
+}  // namespace hphc

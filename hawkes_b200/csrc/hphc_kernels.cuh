@@ -1,0 +1,114 @@
+// Device-side layout and launch interface of the Hawkes pair-sum kernels.
+//
+// Data layout in HBM (one event set of N events, D spatial dimensions):
+//   FP64 records  : N x kF64Stride<D> doubles, {x_0..x_{D-1}, t, pad}, 16-byte rows.
+//   FP32 records  : N x kF32Stride<D> floats,
+//                   {xhi_0..xhi_{D-1}, thi, xlo_0..xlo_{D-1}, tlo, rank, pad},
+//                   16-byte rows; hi = float(v), lo = float(v - hi) so that
+//                   hi + lo carries v to ~2^-48 relative, and rank is the dense
+//                   rank of t (equal times share a rank) stored as int bits, so
+//                   the strict "t_j < t_i" self-excitation mask
+//                   (src/NewHawkes.hpp:540) is an exact integer compare.
+//   tile bounds   : per kTile-event tile, FP64 min and max of t.
+//   partials      : [chunk][6][Npad] FP64 unit pair sums per target event i.
+//   block partials: [block][8] FP64 per-block sums of the per-event
+//                   log-likelihood and gradient contributions.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace hphc {
+
+constexpr int kMaxDim = 8;
+constexpr int kSweepThreads = 128;   // threads per sweep CTA
+constexpr int kTile = 128;           // j events staged in shared memory per step
+constexpr int kFinishThreads = 256;  // threads per finish CTA
+constexpr int kNumAcc = 6;           // unit pair sums per target event
+
+template <int D>
+struct Layout {
+    static constexpr int kF64Stride = ((D + 1) + 1) / 2 * 2;          // doubles per FP64 record
+    static constexpr int kF32Used = 2 * (D + 1) + 1;                   // hi, lo, rank
+    static constexpr int kF32Stride = (kF32Used + 3) / 4 * 4;          // floats per FP32 record
+};
+
+// Per-parameter-vector constants of the pair terms.  Unit terms (no
+// prefactor):  B_u = exp(cA d^2 + cB dt^2) for every pair,
+//              S_u = exp(cS d^2 + cW dt)   for dt > 0,
+// with cA = -a^2/2, cB = -b^2/2, cS = -sigma^2/2, cW = -omega.
+struct PairConsts {
+    double cA, cB, cS, cW;                 // natural-log units (FP64 path)
+    float fAh, fAl, fBh, fBl;              // log2-unit coefficients split hi + lo
+    float fSh, fSl, fWh, fWl;              //   (FP32 path): f = cX*log2(e) = fXh + fXl
+    // Added to every FP32 exponent: -log2(1 + beta), where beta is the mean
+    // relative error of ex2.approx.ftz.f32 measured on the device at engine
+    // creation (the instruction rounds low on average), so the FP32 pair
+    // terms carry no common bias into the sums.
+    float ex2Fix;
+    // Tile-pair underflow skips.  A tile pair is skipped for B when every B_u
+    // in it is exactly zero in the working precision: cA <= 0, cB < 0 and
+    // -cB * min|dt|^2 >= skipB.  Likewise for S with -cW * min(dt) >= skipS.
+    double skipB, skipS;                   // natural-log thresholds; < 0 disables
+};
+
+// Constants of the per-event finish (all FP64).
+struct FinishConsts {
+    double sigma, a, b, omega, theta, mu0;
+    double prefB;     // mu0 a^D b / (2 pi)      : B_ij = prefB * B_u
+    double prefS;     // theta omega sigma^D / sqrt(2 pi) : S_ij = prefS * S_u
+    double bgScale;   // prefB / mu0
+    double seScale;   // prefS / theta
+    double T;         // t[N-1]
+    double constant;  // N (D-1) log(1/sqrt(2 pi))
+    int D;
+};
+
+struct SweepGeometry {
+    int N;            // events
+    int Npad;         // stride of the partials arrays (>= N)
+    int nTiles;       // ceil(N / kTile)
+    int nChunks;      // j-ranges per strip
+    int chunkTiles;   // tiles per j-range
+    int nStrips;      // ceil(N / strip size)
+};
+
+// ---- launchers (return cudaError_t of the launch) ---------------------------
+
+// Pack FP64 locations (N x D row-major) and times into the kernel records and
+// compute per-tile time bounds.  ranks may be null for the FP64 layout.
+cudaError_t launch_pack_f64(int D, int N, const double* loc, const double* times, double* rec,
+                            double* tileMin, double* tileMax, cudaStream_t s);
+cudaError_t launch_pack_f32(int D, int N, const double* loc, const double* times,
+                            const int32_t* ranks, float* rec, double* tileMin, double* tileMax,
+                            cudaStream_t s);
+
+// Pair sweep: fills partials[chunk][6][Npad] with unit pair sums.  R is the
+// number of target events per thread (strip = kSweepThreads * R events).
+cudaError_t launch_sweep_f64(int D, int R, const SweepGeometry& g, const double* rec,
+                             const double* tileMin, const double* tileMax, const PairConsts& c,
+                             double* partials, cudaStream_t s);
+cudaError_t launch_sweep_f32c(int D, int R, const SweepGeometry& g, const float* rec,
+                              const double* tileMin, const double* tileMax, const PairConsts& c,
+                              double* partials, cudaStream_t s);
+
+// Per-event finish: combines the chunk partials of each event in chunk order,
+// forms lambda_i, the log-likelihood and gradient contributions and (if probs
+// is non-null) P_i, and writes one 8-double block sum per finish CTA.
+cudaError_t launch_finish(const SweepGeometry& g, const double* partials, const double* times,
+                          const FinishConsts& f, double* blockSums, double* probs,
+                          cudaStream_t s);
+
+// Fixed-order reduction of the block sums: out[0] = log-likelihood (with the
+// constant), out[1..6] = gradient.
+cudaError_t launch_final(int nBlocks, const double* blockSums, const FinishConsts& f, double* out,
+                         cudaStream_t s);
+
+// Calibration of the FP32 exponential: writes ceil(n / kFinishThreads) CTA
+// sums of (ex2.approx(x) / 2^x - 1) for n arguments spread over [-16, 0).
+cudaError_t launch_ex2_bias(int n, double* blockSums, cudaStream_t s);
+
+// Number of finish CTAs for N events.
+inline int finish_blocks(int N) { return (N + kFinishThreads - 1) / kFinishThreads; }
+
+}  // namespace hphc

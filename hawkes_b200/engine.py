@@ -1,0 +1,327 @@
+"""Python host interface of the B200 Hawkes likelihood engine.
+
+Two layers, both thin wrappers over the C ABI in include/hphc.h:
+
+* :class:`CudaHawkes` mirrors the reference engine interface
+  ``hph::AbstractHawkes`` (src/AbstractHawkes.hpp:32-60) method for method:
+  ``setTimesData``, ``updateLocations``, ``setParameters``,
+  ``getSumOfLikContribs``, ``getLogLikelihoodGradient`` (commented out in the
+  reference at src/AbstractHawkes.hpp:44), ``getProbsSelfExcite``,
+  ``storeState``/``restoreState``/``acceptState`` and
+  ``getInternalDimension``.  Construction mirrors ``hph::factory``
+  (src/factory.cpp:32) with the GPU slot selected.
+
+* Module functions mirror the reference's R API (R/hph.R:10-110,
+  src/hpHawkes.cpp:59-151): ``createEngine``, ``setTimesData``,
+  ``updateLocations`` (an N x D matrix, row-major as R/hph.R:103 arranges it),
+  ``setParameters``, ``getLogLikelihood``, ``getProbsSelfExcite`` and the
+  gradient the reference does not expose.  They raise the same messages as the
+  R functions ("locations not set", "times not set", "parameters not set",
+  "Invalid data size").
+
+Every call goes to the CUDA library; errors raise :class:`HawkesError` with the
+engine's message.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional
+
+import numpy as np
+
+from . import _native
+
+_lib = _native.lib
+_dp = ctypes.POINTER(ctypes.c_double)
+
+# hph::Flags (src/flags.h:6-13) and the two bits added for the CUDA engine.
+FLOAT = 1 << 2
+TBB = 1 << 3
+OPENCL = 1 << 4
+SSE = 1 << 5
+AVX = 1 << 6
+AVX512 = 1 << 7
+CUDA = 1 << 8
+COMPENSATED = 1 << 9
+NO_UNDERFLOW_SKIP = 1 << 10
+
+PRECISION_FP64 = 0
+PRECISION_FP32_COMP = 1
+
+# Parameter order of NewHawkes::setParameters (src/NewHawkes.hpp:331-339).
+PARAMETER_NAMES = ("sigmaXprec", "tauXprec", "tauTprec", "omega", "theta", "mu0")
+
+
+class HawkesError(RuntimeError):
+    """A non-zero status from the CUDA engine."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(message)
+        self.status = status
+
+
+def _as_f64(a, name: str) -> np.ndarray:
+    arr = np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(-1))
+    return arr
+
+
+class CudaHawkes:
+    """The CUDA engine behind the reference's ``hph::AbstractHawkes`` interface."""
+
+    def __init__(self, embeddingDimension: int, locationCount: int, flags: int = CUDA,
+                 device: int = 0):
+        h = ctypes.c_void_p()
+        st = _lib.hphc_create(int(embeddingDimension), int(locationCount), int(flags),
+                              int(device), ctypes.byref(h))
+        if st != 0:
+            raise HawkesError(st, "hphc_create: " + _lib.hphc_status_string(st).decode())
+        self._h = h
+        self.embeddingDimension = int(embeddingDimension)
+        self.locationCount = int(locationCount)
+        self.flags = int(flags)
+
+    # -- plumbing -------------------------------------------------------------
+    def _check(self, st: int, what: str) -> None:
+        if st != 0:
+            msg = _lib.hphc_last_error(self._h).decode() or _lib.hphc_status_string(st).decode()
+            raise HawkesError(st, f"{what}: {msg}")
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            _lib.hphc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- hph::AbstractHawkes ----------------------------------------------------
+    def setTimesData(self, data) -> None:
+        arr = _as_f64(data, "times")
+        self._check(_lib.hphc_set_times_data(self._h, arr.ctypes.data_as(_dp), arr.size),
+                    "setTimesData")
+
+    def updateLocations(self, locationIndex: int, location) -> None:
+        arr = _as_f64(location, "locations")
+        self._check(_lib.hphc_update_locations(self._h, int(locationIndex),
+                                               arr.ctypes.data_as(_dp), arr.size),
+                    "updateLocations")
+
+    def setParameters(self, data) -> None:
+        arr = _as_f64(data, "parameters")
+        self._check(_lib.hphc_set_parameters(self._h, arr.ctypes.data_as(_dp), arr.size),
+                    "setParameters")
+
+    def getSumOfLikContribs(self) -> float:
+        out = ctypes.c_double()
+        self._check(_lib.hphc_get_sum_of_lik_contribs(self._h, ctypes.byref(out)),
+                    "getSumOfLikContribs")
+        return out.value
+
+    def getLogLikelihoodGradient(self) -> np.ndarray:
+        out = np.zeros(6)
+        self._check(_lib.hphc_get_log_likelihood_gradient(self._h, out.ctypes.data_as(_dp), 6),
+                    "getLogLikelihoodGradient")
+        return out
+
+    def getLogLikelihoodAndGradient(self):
+        ll = ctypes.c_double()
+        g = np.zeros(6)
+        self._check(_lib.hphc_get_log_likelihood_and_gradient(self._h, ctypes.byref(ll),
+                                                              g.ctypes.data_as(_dp), 6),
+                    "getLogLikelihoodAndGradient")
+        return ll.value, g
+
+    def getProbsSelfExcite(self) -> np.ndarray:
+        out = np.zeros(self.locationCount)
+        self._check(_lib.hphc_get_probs_self_excite(self._h, out.ctypes.data_as(_dp), out.size),
+                    "getProbsSelfExcite")
+        return out
+
+    def storeState(self) -> None:
+        self._check(_lib.hphc_store_state(self._h), "storeState")
+
+    def restoreState(self) -> None:
+        self._check(_lib.hphc_restore_state(self._h), "restoreState")
+
+    def acceptState(self) -> None:
+        self._check(_lib.hphc_accept_state(self._h), "acceptState")
+
+    def getInternalDimension(self) -> int:
+        out = ctypes.c_int()
+        self._check(_lib.hphc_get_internal_dimension(self._h, ctypes.byref(out)),
+                    "getInternalDimension")
+        return out.value
+
+    # -- additions ------------------------------------------------------------
+    def batchLogLikelihoodAndGradient(self, params):
+        """Log-likelihood and gradient for K parameter vectors (K x 6)."""
+        p = np.ascontiguousarray(np.asarray(params, dtype=np.float64).reshape(-1, 6))
+        K = p.shape[0]
+        ll = np.zeros(K)
+        g = np.zeros((K, 6))
+        self._check(_lib.hphc_batch_log_likelihood_and_gradient(
+            self._h, p.ctypes.data_as(_dp), K, ll.ctypes.data_as(_dp), g.ctypes.data_as(_dp)),
+            "batchLogLikelihoodAndGradient")
+        return ll, g
+
+    @property
+    def precision(self) -> int:
+        out = ctypes.c_int()
+        self._check(_lib.hphc_get_precision(self._h, ctypes.byref(out)), "getPrecision")
+        return out.value
+
+    @property
+    def stream(self) -> int:
+        """The engine's cudaStream_t as an integer handle."""
+        out = ctypes.c_void_p()
+        self._check(_lib.hphc_get_stream(self._h, ctypes.byref(out)), "getStream")
+        return int(out.value or 0)
+
+    def enqueueLogLikelihoodAndGradient(self) -> None:
+        self._check(_lib.hphc_enqueue_log_likelihood_and_gradient(self._h),
+                    "enqueueLogLikelihoodAndGradient")
+
+    def readResults(self):
+        ll = ctypes.c_double()
+        g = np.zeros(6)
+        self._check(_lib.hphc_read_results(self._h, ctypes.byref(ll), g.ctypes.data_as(_dp), 6),
+                    "readResults")
+        return ll.value, g
+
+    def setKernelTiming(self, enable: bool = True) -> None:
+        self._check(_lib.hphc_set_kernel_timing(self._h, int(bool(enable))), "setKernelTiming")
+
+    def kernelTimes(self):
+        """(sweep ms, finish ms) of the last evaluation made with kernel timing on."""
+        a = ctypes.c_float()
+        b = ctypes.c_float()
+        self._check(_lib.hphc_get_kernel_times(self._h, ctypes.byref(a), ctypes.byref(b)),
+                    "kernelTimes")
+        return a.value, b.value
+
+    def lastLaunchStats(self):
+        """(kernel launches, background terms evaluated, self-excitation terms
+        evaluated) of the last evaluation."""
+        n = ctypes.c_int()
+        nb = ctypes.c_double()
+        ns = ctypes.c_double()
+        self._check(_lib.hphc_get_last_launch_stats(self._h, ctypes.byref(n), ctypes.byref(nb),
+                                                    ctypes.byref(ns)), "lastLaunchStats")
+        return n.value, nb.value, ns.value
+
+
+def factory(embeddingDimension: int, locationCount: int, flags: int, device: int = 0,
+            threads: int = 0) -> CudaHawkes:
+    """``hph::factory`` (src/factory.cpp:32) restricted to its GPU slot.
+
+    ``OPENCL`` or ``CUDA`` in flags selects the CUDA engine; ``FLOAT`` (the
+    reference's single-precision request) selects the FP32-compensated mode.
+    ``threads`` is accepted for signature compatibility and ignored.
+    """
+    if not flags & (OPENCL | CUDA):
+        raise HawkesError(5, "factory: this package provides only the GPU engine; "
+                             "set the OPENCL or CUDA flag")
+    return CudaHawkes(embeddingDimension, locationCount, flags | CUDA, device)
+
+
+# ---------------------------------------------------------------- R mirror --
+
+class Engine(dict):
+    """The list ``createEngine`` returns in R (src/hpHawkes.cpp:97-106)."""
+
+
+def createEngine(embeddingDimension: int, locationCount: int, tbb: int = 0, simd: int = 0,
+                 gpu: int = 1, single: bool = False) -> Engine:
+    """``createEngine`` (src/hpHawkes.cpp:59-109) with the GPU path selected.
+
+    ``gpu`` is the device number as in the R glue (``deviceNumber = gpu``,
+    src/hpHawkes.cpp:68); out-of-range numbers fall back to device 0 as the
+    OpenCL engine falls back to the default device.  ``single`` selects the
+    FP32-compensated mode.
+    """
+    if gpu <= 0:
+        raise HawkesError(5, "createEngine: the CUDA engine needs gpu > 0")
+    flags = OPENCL | CUDA
+    if single:
+        flags |= FLOAT
+    eng = CudaHawkes(embeddingDimension, locationCount, flags, gpu)
+    return Engine(engine=eng, embeddingDimension=embeddingDimension,
+                  locationCount=locationCount, timesInitialized=False,
+                  locationsInitialized=False, threads=0, deviceNumber=gpu, flags=flags,
+                  parameters=None)
+
+
+def updateLocations(engine: Engine, locations) -> Engine:
+    """R/hph.R:102-110: an N x D matrix, sent row-major."""
+    loc = np.asarray(locations, dtype=np.float64)
+    flat = np.ascontiguousarray(loc).reshape(-1)
+    if flat.size != engine["locationCount"] * engine["embeddingDimension"]:
+        raise HawkesError(2, "Invalid data size")
+    engine["engine"].updateLocations(-1, flat)
+    engine["locationsInitialized"] = True
+    return engine
+
+
+def setTimesData(engine: Engine, data) -> Engine:
+    """R/hph.R:83-91."""
+    t = np.asarray(data, dtype=np.float64).reshape(-1)
+    if t.size != engine["locationCount"]:
+        raise HawkesError(2, "Invalid data size")
+    engine["engine"].setTimesData(t)
+    engine["timesInitialized"] = True
+    return engine
+
+
+def setParameters(engine: Engine, parameters) -> Engine:
+    """R/hph.R:68-72."""
+    engine["engine"].setParameters(parameters)
+    engine["parameters"] = np.asarray(parameters, dtype=np.float64).copy()
+    return engine
+
+
+def _check_ready(engine: Engine) -> None:
+    # R/hph.R:12-22
+    if not engine["locationsInitialized"]:
+        raise HawkesError(7, "locations not set")
+    if not engine["timesInitialized"]:
+        raise HawkesError(7, "times not set")
+    if engine.get("parameters") is None:
+        raise HawkesError(7, "parameters not set")
+
+
+def getLogLikelihood(engine: Engine) -> float:
+    """R/hph.R:10-31."""
+    _check_ready(engine)
+    return engine["engine"].getSumOfLikContribs()
+
+
+def getProbsSelfExcite(engine: Engine) -> np.ndarray:
+    """R/hph.R:41-57."""
+    _check_ready(engine)
+    return engine["engine"].getProbsSelfExcite()
+
+
+def getGradient(engine: Engine) -> np.ndarray:
+    """Gradient of the log-likelihood (the reference's commented-out
+    ``.getLogLikelihoodGradient``, src/hpHawkes.cpp:124-130)."""
+    _check_ready(engine)
+    return engine["engine"].getLogLikelihoodGradient()
+
+
+def engineInitial(locations, N: int, P: int, times, parameters, threads: int = 0, simd: int = 0,
+                  gpu: int = 1, single: bool = False) -> Engine:
+    """R/Untitled.R:193-212: create, set locations, times and parameters."""
+    engine = createEngine(P, N, threads, simd, gpu, single)
+    engine = updateLocations(engine, locations)
+    engine = setTimesData(engine, times)
+    engine = setParameters(engine, parameters)
+    return engine

@@ -1,0 +1,198 @@
+/*
+ * hphc.h -- C ABI of the B200 CUDA Hawkes likelihood engine (libhawkes_b200.so).
+ *
+ * The engine evaluates the O(N^2) spatio-temporal Hawkes log-likelihood of
+ * hpHawkes, its analytic parameter gradient and the per-event
+ * self-excitation probabilities on one NVIDIA B200 (sm_100a).  These entry
+ * points are what a binding of the reference's engine interface
+ * hph::AbstractHawkes (src/AbstractHawkes.hpp:32-60) calls: the header-only
+ * adapter include/hawkes_b200/CudaHawkes.hpp wraps them in a class deriving
+ * from hph::AbstractHawkes, and Rcpp / JNI / ctypes bindings can call them
+ * directly.
+ *
+ * Conventions
+ *   - Every function returns an int status (HPHC_OK = 0).  On failure the
+ *     handle keeps a message, read with hphc_last_error().  The reference
+ *     reports errors with assert (compiled out), Rcpp::stop or exit(-1); the C
+ *     ABI reports them instead of stopping the process.
+ *   - The caller owns every pointer passed in; inputs are copied into the
+ *     engine before the call returns and outputs are written before it
+ *     returns (synchronous, like the reference's bufferedCopy,
+ *     src/MemoryManagement.hpp:40-56).
+ *   - An engine is not thread-safe: one caller thread per handle, as with the
+ *     reference engines.  Separate handles may be used from separate threads.
+ *   - Parameter vectors have 6 entries in the reference order
+ *     (src/NewHawkes.hpp:331-339): sigma (sigmaXprec), a (tauXprec),
+ *     b (tauTprec), omega, theta, mu0.  sigma, a and b are precisions.
+ *   - Gradients have the same 6 entries, d logL / d p_k.
+ */
+#ifndef HPHC_H
+#define HPHC_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define HPHC_OK 0
+#define HPHC_ERR_INVALID_HANDLE 1   /* null or destroyed handle                        */
+#define HPHC_ERR_BAD_LENGTH 2       /* a length does not match N, D or 6               */
+#define HPHC_ERR_BAD_ARGUMENT 3     /* null pointer, index out of range, N < 1 ...     */
+#define HPHC_ERR_NONFINITE 4        /* NaN or infinity in times or locations           */
+#define HPHC_ERR_UNSUPPORTED 5      /* D outside 1..8, unknown precision flags         */
+#define HPHC_ERR_CUDA 6             /* a CUDA runtime call or kernel launch failed     */
+#define HPHC_ERR_NOT_READY 7        /* times, locations or parameters not set yet     */
+#define HPHC_ERR_DEVICE_TIMEOUT 8   /* a bounded device-side wait gave up              */
+#define HPHC_ERR_NO_DEVICE 9        /* no CUDA device visible                          */
+#define HPHC_ERR_OUT_OF_MEMORY 10   /* device or pinned host allocation failed         */
+#define HPHC_ERR_SCRATCH_TOO_SMALL 11 /* a problem needs more scratch than provided    */
+
+/* ---- flags: bit-compatible with hph::Flags (src/flags.h:6-13) ----------- */
+#define HPHC_FLAG_FLOAT (1L << 2)     /* single precision: FP32-compensated pair math */
+#define HPHC_FLAG_TBB (1L << 3)       /* accepted and ignored (CPU threading flag)    */
+#define HPHC_FLAG_OPENCL (1L << 4)    /* accepted: the GPU engine slot                */
+#define HPHC_FLAG_SSE (1L << 5)       /* accepted and ignored                         */
+#define HPHC_FLAG_AVX (1L << 6)       /* accepted and ignored                         */
+#define HPHC_FLAG_AVX512 (1L << 7)    /* accepted and ignored                         */
+#define HPHC_FLAG_CUDA (1L << 8)      /* new: select the CUDA engine                  */
+#define HPHC_FLAG_COMPENSATED (1L << 9) /* new: FP32 pair terms, compensated, FP64 reductions */
+#define HPHC_FLAG_NO_UNDERFLOW_SKIP (1L << 10) /* new: evaluate every tile pair, even those
+                                                  whose terms all underflow to zero */
+
+/* Precision modes reported by hphc_get_precision(). */
+#define HPHC_PRECISION_FP64 0          /* plain FP64 pair terms and reductions           */
+#define HPHC_PRECISION_FP32_COMP 1     /* FP32 pair terms, compensated; FP64 reductions  */
+
+typedef struct hphc_engine hphc_engine;
+
+/* ---- lifetime ----------------------------------------------------------- */
+
+/*
+ * Create an engine for locationCount events in embeddingDimension (1..8)
+ * spatial dimensions.  Replaces hph::factory (src/factory.cpp:32) for the GPU
+ * slot and the OpenCLHawkes constructor (src/backend/opencl/instantiate.cpp:15-52).
+ * flags: HPHC_FLAG_FLOAT or HPHC_FLAG_COMPENSATED select the FP32-compensated
+ * mode, otherwise plain FP64.  device: CUDA device ordinal; a value < 0 or
+ * beyond the device count selects device 0, as the OpenCL engine falls back to
+ * the default device (src/backend/opencl/OpenCLHawkes.hpp:88-92).
+ */
+int hphc_create(int embeddingDimension, int locationCount, long flags, int device,
+                hphc_engine** out);
+
+/* Release every device and host resource of the engine.  Null is a no-op. */
+void hphc_destroy(hphc_engine* engine);
+
+/* Message of the last failed call on this handle ("" if none). */
+const char* hphc_last_error(const hphc_engine* engine);
+
+/* Fixed text for a status code. */
+const char* hphc_status_string(int status);
+
+/* ---- data and parameters (hph::AbstractHawkes) ------------------------- */
+
+/* Replaces AbstractHawkes::setTimesData (src/AbstractHawkes.hpp:49;
+ * src/NewHawkes.hpp:320-323).  length must equal N.  Times need not be sorted;
+ * as in the reference, T = data[N-1]. */
+int hphc_set_times_data(hphc_engine* engine, const double* data, size_t length);
+
+/* Replaces AbstractHawkes::updateLocations (src/AbstractHawkes.hpp:43;
+ * src/NewHawkes.hpp:244-276).  locationIndex == -1: all N rows, row-major,
+ * length == D*N.  Otherwise one row, length == D. */
+int hphc_update_locations(hphc_engine* engine, int locationIndex, const double* location,
+                          size_t length);
+
+/* Replaces AbstractHawkes::setParameters (src/AbstractHawkes.hpp:50;
+ * src/NewHawkes.hpp:331-339).  length must be 6. */
+int hphc_set_parameters(hphc_engine* engine, const double* data, size_t length);
+
+/* ---- evaluation --------------------------------------------------------- */
+
+/* Replaces AbstractHawkes::getSumOfLikContribs (src/AbstractHawkes.hpp:42;
+ * src/NewHawkes.hpp:278-282, :636-660): the full log-likelihood, including
+ * the N(D-1)log(1/sqrt(2 pi)) constant. */
+int hphc_get_sum_of_lik_contribs(hphc_engine* engine, double* out);
+
+/* The interface method the reference leaves commented out
+ * (src/AbstractHawkes.hpp:44, src/NewHawkes.hpp:341-345): d logL / d p, 6
+ * entries in parameter order.  length must be 6. */
+int hphc_get_log_likelihood_gradient(hphc_engine* engine, double* out, size_t length);
+
+/* Log-likelihood and gradient from one pair sweep.  No reference
+ * counterpart as a single call; equals getSumOfLikContribs followed by
+ * getLogLikelihoodGradient on the same state.  gradient may be null. */
+int hphc_get_log_likelihood_and_gradient(hphc_engine* engine, double* loglik, double* gradient,
+                                         size_t length);
+
+/* Replaces AbstractHawkes::getProbsSelfExcite (src/AbstractHawkes.hpp:45;
+ * src/NewHawkes.hpp:325-329, :662-719).  length must equal N. */
+int hphc_get_probs_self_excite(hphc_engine* engine, double* out, size_t length);
+
+/* ---- MCMC state (src/AbstractHawkes.hpp:46-48) ------------------------ */
+
+/* Save parameters, locations and the last log-likelihood.  The reference's
+ * NewHawkes::storeState copies in the wrong direction (src/NewHawkes.hpp:286-291);
+ * this saves the current state, as OpenCLHawkes::storeState does
+ * (src/backend/opencl/OpenCLHawkes.hpp:283-300). */
+int hphc_store_state(hphc_engine* engine);
+
+/* Return to the saved state (src/NewHawkes.hpp:305-318).  The saved
+ * locations are used by every later evaluation (the OpenCL engine kept
+ * binding the unswapped buffer, src/backend/opencl/OpenCLHawkes.hpp:257, :382). */
+int hphc_restore_state(hphc_engine* engine);
+
+/* Accept the proposal (src/NewHawkes.hpp:297-303): keeps the current state. */
+int hphc_accept_state(hphc_engine* engine);
+
+/* Replaces AbstractHawkes::getInternalDimension (src/AbstractHawkes.hpp:51): D. */
+int hphc_get_internal_dimension(hphc_engine* engine, int* out);
+
+/* ---- batched evaluation (no reference counterpart) ---------------------
+ *
+ * Evaluate K parameter vectors (K x 6, row-major) on the engine's events in
+ * one launch sequence.  loglik has K entries; gradient (K x 6) may be null.
+ * The engine's own parameters and cached results are not changed. */
+int hphc_batch_log_likelihood_and_gradient(hphc_engine* engine, const double* params, int K,
+                                           double* loglik, double* gradient);
+
+/* ---- introspection and device-resident timing --------------------------- */
+
+/* Precision mode in use (HPHC_PRECISION_*). */
+int hphc_get_precision(hphc_engine* engine, int* out);
+
+/* The cudaStream_t the engine launches on, as void*.  Callers may record CUDA
+ * events on it to time the device work of hphc_enqueue_*. */
+int hphc_get_stream(hphc_engine* engine, void** stream);
+
+/* Enqueue one log-likelihood + gradient evaluation on the engine's stream
+ * with the data already on the device, without waiting and without copying
+ * results back.  hphc_read_results() waits and returns them. */
+int hphc_enqueue_log_likelihood_and_gradient(hphc_engine* engine);
+
+/* Wait for the last enqueued evaluation and copy its log-likelihood and
+ * gradient (6, may be null) to the host. */
+int hphc_read_results(hphc_engine* engine, double* loglik, double* gradient, size_t length);
+
+/* Kernel launches made by the most recent evaluation call (for launch
+ * accounting), and how many background and self-excitation pair terms its
+ * sweep evaluated.  Of the 2 N^2 possible terms the rest were skipped at tile
+ * level: the non-causal half of the self-excitation sum and tile pairs whose
+ * terms all underflow to exactly zero in the working precision. */
+int hphc_get_last_launch_stats(hphc_engine* engine, int* kernelLaunches,
+                               double* backgroundTerms, double* selfExciteTerms);
+
+/* Record CUDA events around the pair-sweep kernel and around the finish
+ * kernels of every later evaluation (enable != 0), on the engine's stream. */
+int hphc_set_kernel_timing(hphc_engine* engine, int enable);
+
+/* Device durations (ms) of the pair sweep and of the finish + final kernels
+ * of the most recent evaluation made with kernel timing enabled.  Waits for
+ * that evaluation to finish. */
+int hphc_get_kernel_times(hphc_engine* engine, float* sweepMs, float* finishMs);
+
+#ifdef __cplusplus
+}  /* extern "C" */
+#endif
+
+#endif /* HPHC_H */

@@ -1,0 +1,206 @@
+"""GPU parity tests: the CUDA engine (through the C ABI) against the reference
+engine's outputs (golden fixtures) and the oracle.
+
+Tolerances
+  FP64 plain        log-likelihood relative 1e-10; probabilities 1e-10 absolute;
+                    gradient 1e-10 of its absolute scale (sum over events of
+                    |per-event contribution|, per component).
+  FP32-compensated  at the small fixture sizes: log-likelihood relative 1e-7,
+                    gradient 1e-6 of its term-level scale (sum over events of
+                    |each additive term| of the contribution, e.g.
+                    |D/sigma S_i| + |sigma S_i d^2|), probabilities 2e-5 absolute.
+                    (The 1e-8 target is checked at N=50,000 in
+                    test_accuracy_gpu.py.)
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+import hawkes_b200 as hb
+import oracle
+from hawkes_b200 import workloads
+
+pytestmark = pytest.mark.gpu
+
+FP64 = hb.CUDA
+FP32C = hb.CUDA | hb.COMPENSATED
+TOL = {FP64: dict(ll=1e-10, grad=1e-10, probs=1e-10),
+       FP32C: dict(ll=1e-7, grad=1e-6, probs=2e-5)}
+
+
+def engine(loc, t, p, flags):
+    loc = np.asarray(loc, dtype=np.float64)
+    e = hb.CudaHawkes(loc.shape[1], loc.shape[0], flags, 0)
+    e.setTimesData(t)
+    e.updateLocations(-1, loc.reshape(-1))
+    e.setParameters(p)
+    return e
+
+
+def check_case(name, c, flags):
+    tol = TOL[flags]
+    with engine(c["loc"], c["t"], c["params"], flags) as e:
+        ll, g = e.getLogLikelihoodAndGradient()
+        probs = e.getProbsSelfExcite()
+        ll2 = e.getSumOfLikContribs()
+        g2 = e.getLogLikelihoodGradient()
+    ref = float(c["ref_loglik"])
+    assert abs(ll - ref) <= tol["ll"] * abs(ref), (name, ll, ref)
+    assert ll == ll2 and np.array_equal(g, g2), name
+    # FP64: against the per-event scale; FP32: against the term-level scale
+    # (the condition scale of the sum, which is what FP32 pair terms resolve)
+    key = "grad_scale" if flags == FP64 else "grad_term_scale"
+    scale = np.maximum(c[key], 1e-300)
+    if flags != FP64:
+        # FP32 flushes pair terms below 2^-126 to zero, so a component whose
+        # whole magnitude sits near that range (e.g. d logL/d sigma ~ 1e-23 in
+        # the 8-D case, next to components ~1e4) is resolved only to an
+        # absolute floor far below the gradient's size.
+        scale = scale + 1e-14 * np.max(c[key]) / tol["grad"]
+    gerr = np.abs(g - c["oracle_grad"]) / scale
+    assert np.all(gerr <= tol["grad"]), (name, gerr)
+    perr = np.max(np.abs(probs - c["ref_probs"]))
+    assert perr <= tol["probs"], (name, perr)
+
+
+@pytest.mark.parametrize("flags", [FP64, FP32C], ids=["fp64", "fp32c"])
+def test_golden_synthetic(golden_synthetic, flags):
+    for name, c in sorted(golden_synthetic.items()):
+        check_case(name, c, flags)
+
+
+@pytest.mark.parametrize("flags", [FP64, FP32C], ids=["fp64", "fp32c"])
+def test_golden_dcdata(golden_dcdata, flags):
+    for name, c in sorted(golden_dcdata.items()):
+        check_case(name, c, flags)
+
+
+@pytest.mark.parametrize("flags", [FP64, FP32C], ids=["fp64", "fp32c"])
+def test_random_cases_against_oracle(flags):
+    rng = np.random.default_rng(2024)
+    for trial in range(6):
+        D = int(rng.integers(1, 9))
+        N = int(rng.integers(1, 1500))
+        loc = rng.uniform(0, 15, size=(N, D))
+        t = np.sort(rng.uniform(0, 3000, size=N))
+        p = workloads.BASE_PARAMS * np.exp(0.4 * rng.standard_normal(6))
+        o = oracle.oracle_eval(loc, t, p, threads=8)
+        c = {"loc": loc, "t": t, "params": p, "ref_loglik": o["loglik"],
+             "ref_probs": o["probs"], "oracle_grad": o["grad"], "grad_scale": o["grad_scale"],
+             "grad_term_scale": o["grad_term_scale"]}
+        check_case(f"trial{trial}_D{D}_N{N}", c, flags)
+
+
+@pytest.mark.parametrize("flags", [FP64, FP32C], ids=["fp64", "fp32c"])
+def test_underflow_skip_is_bit_exact(flags):
+    # Tile pairs whose terms all underflow are skipped; evaluating them anyway
+    # must give identical bits.
+    loc, t = workloads.uniform(20000, seed=7)
+    p = workloads.BASE_PARAMS
+    with engine(loc, t, p, flags) as a, engine(loc, t, p, flags | hb.NO_UNDERFLOW_SKIP) as b:
+        la, ga = a.getLogLikelihoodAndGradient()
+        lb, gb = b.getLogLikelihoodAndGradient()
+        pa, pb = a.getProbsSelfExcite(), b.getProbsSelfExcite()
+        _, nba, nsa = a.lastLaunchStats()
+        _, nbb, nsb = b.lastLaunchStats()
+    assert la == lb and np.array_equal(ga, gb) and np.array_equal(pa, pb)
+    assert nba + nsa < nbb + nsb  # the skip did remove work
+    assert nbb == 20000.0 ** 2  # without it every background term is evaluated
+
+
+@pytest.mark.parametrize("flags", [FP64, FP32C], ids=["fp64", "fp32c"])
+def test_repeatable_bits(flags):
+    loc, t = workloads.uniform(5000, seed=8)
+    with engine(loc, t, workloads.BASE_PARAMS, flags) as e:
+        r1 = e.getLogLikelihoodAndGradient()
+        r2 = e.getLogLikelihoodAndGradient()
+    assert r1[0] == r2[0] and np.array_equal(r1[1], r2[1])
+
+
+def test_single_row_updates_equal_full_update():
+    loc, t = workloads.uniform(777, seed=9)
+    p = workloads.BASE_PARAMS
+    with engine(loc, t, p, FP64) as full:
+        want = full.getLogLikelihoodAndGradient()
+    e = hb.CudaHawkes(2, 777, FP64, 0)
+    e.setTimesData(t)
+    for i in range(777):  # as the reference CLI does (src/benchmark.cpp:167-171)
+        e.updateLocations(i, loc[i])
+    e.setParameters(p)
+    got = e.getLogLikelihoodAndGradient()
+    e.close()
+    assert got[0] == want[0] and np.array_equal(got[1], want[1])
+
+
+@pytest.mark.parametrize("flags", [FP64, FP32C], ids=["fp64", "fp32c"])
+def test_store_restore_state(flags):
+    loc, t = workloads.uniform(3000, seed=10)
+    p = workloads.BASE_PARAMS
+    with engine(loc, t, p, flags) as e:
+        first = e.getLogLikelihoodAndGradient()
+        e.storeState()
+        moved = loc.copy()
+        moved[17] += 0.5
+        e.updateLocations(17, moved[17])
+        e.setParameters(p * 1.1)
+        second = e.getLogLikelihoodAndGradient()
+        assert second[0] != first[0]
+        e.restoreState()
+        third = e.getLogLikelihoodAndGradient()
+        assert third[0] == first[0] and np.array_equal(third[1], first[1])
+        e.acceptState()
+        e.storeState()
+        e.updateLocations(-1, moved)
+        e.acceptState()  # keep the proposal
+        fourth = e.getLogLikelihoodAndGradient()
+    with engine(moved, t, p, flags) as f:
+        assert f.getLogLikelihoodAndGradient()[0] == fourth[0]
+
+
+def test_batch_equals_single_evaluations():
+    loc, t = workloads.uniform(4000, seed=12)
+    P = workloads.proposals(5, seed=13)
+    with engine(loc, t, workloads.BASE_PARAMS, FP32C) as e:
+        ll, g = e.batchLogLikelihoodAndGradient(P)
+        for k in range(5):
+            e.setParameters(P[k])
+            lk, gk = e.getLogLikelihoodAndGradient()
+            assert lk == ll[k] and np.array_equal(gk, g[k])
+
+
+def test_argument_errors_on_a_live_engine():
+    with hb.CudaHawkes(2, 10, FP64, 0) as e:
+        with pytest.raises(hb.HawkesError) as ei:
+            e.setTimesData(np.zeros(9))
+        assert ei.value.status == 2
+        with pytest.raises(hb.HawkesError) as ei:
+            e.updateLocations(-1, np.zeros(19))
+        assert ei.value.status == 2
+        with pytest.raises(hb.HawkesError) as ei:
+            e.updateLocations(10, np.zeros(2))
+        assert ei.value.status == 3
+        with pytest.raises(hb.HawkesError) as ei:
+            e.setParameters(np.ones(5))
+        assert ei.value.status == 2
+        bad = np.zeros(10)
+        bad[3] = np.nan
+        with pytest.raises(hb.HawkesError) as ei:
+            e.setTimesData(bad)
+        assert ei.value.status == 4
+        assert e.getInternalDimension() == 2
+
+
+def test_r_mirror_call_sequence():
+    # The sequence R's engineInitial / getLogLikelihood / getProbsSelfExcite
+    # make (R/Untitled.R:193-212, R/hph.R:10-57), through the Python mirror.
+    loc, t = workloads.uniform(600, seed=14)
+    eng = hb.createEngine(2, 600, gpu=1, single=False)
+    with pytest.raises(hb.HawkesError, match="locations not set"):
+        hb.getLogLikelihood(eng)
+    eng = hb.engineInitial(loc, 600, 2, t, workloads.BASE_PARAMS)
+    o = oracle.oracle_eval(loc, t, workloads.BASE_PARAMS, threads=4)
+    assert abs(hb.getLogLikelihood(eng) - o["loglik"]) <= 1e-10 * abs(o["loglik"])
+    assert np.max(np.abs(hb.getProbsSelfExcite(eng) - o["probs"])) <= 1e-10
+    g = hb.getGradient(eng)
+    assert np.all(np.abs(g - o["grad"]) <= 1e-10 * o["grad_scale"])
