@@ -147,7 +147,9 @@ def reference_arm(args):
         print(json.dumps({"impl": "reference",
                           "unavailable": "reference CPU engine (oracle/_ref) not built"}))
         return 0
-    # Calibrate the sample size so one step takes ~6 s on this host.
+    # Calibrate the sample size so the whole run (warm-up + steps) takes about
+    # two minutes on this host, and no step more than ~6 s.
+    step_s = min(6.0, 120.0 / max(1, args.steps + args.warmup))
     loc, t = workloads.uniform(4000, seed=SEED)
     eng = oracle.RefEngine(2, 4000, threads=cores)
     eng.set_data(loc, t)
@@ -156,7 +158,7 @@ def reference_arm(args):
     eng.loglik()
     rate = 4000.0 ** 2 / (time.perf_counter() - t0)
     eng.close()
-    n = int(min(N_EVENTS, max(4000, math.sqrt(6.0 * rate)) // 1000 * 1000))
+    n = int(min(N_EVENTS, max(2000, math.sqrt(step_s * rate)) // 1000 * 1000))
     loc, t = workloads.uniform(n, seed=SEED)
     eng = oracle.RefEngine(2, n, threads=cores)
     variant = eng.variant.splitlines()[0]
@@ -319,6 +321,7 @@ def ours_arm(args):
         ms32, sweep32, res32 = time_device(fp32, args.steps, args.warmup, torch, s32, flush)
         barrier()
     launches, nb, ns = fp32.lastLaunchStats()
+    shape32 = fp32.sweepShape()
     _, nb64, ns64 = fp64.lastLaunchStats()
 
     tot32 = torch.tensor([sum(ms32), sum(ms64)], dtype=torch.float64, device=f"cuda:{local}")
@@ -382,7 +385,8 @@ def ours_arm(args):
                   "note": "pair terms the sweep evaluated; the rest are the non-causal half of "
                           "the self-excitation sum and tile pairs whose terms are all exactly "
                           "zero in FP32"},
-        "roofline": {"bound": "fp32", "kernel": "sweep_f32c_kernel<2,2>",
+        "roofline": {"bound": "fp32",
+                     "kernel": f"sweep_f32c_kernel<D=2, R={shape32[0]}>, {shape32[1]} items/SM",
                      "achieved": achieved, "peak": peak_inst, "unit": "Tinst/s",
                      "frac": achieved / peak_inst, "traffic": traffic,
                      "count": "FP32-pipe instructions, FMA = 1: 11 per background term + 5 per "
@@ -405,7 +409,7 @@ def ours_arm(args):
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--n", type=int, default=N_EVENTS, help=argparse.SUPPRESS)

@@ -43,6 +43,8 @@ SIGNATURES = {
     "hphc_read_results": (ctypes.c_int, [_handle, _c_double_p, _c_double_p, ctypes.c_size_t]),
     "hphc_get_last_launch_stats": (ctypes.c_int, [_handle, _c_int_p, _c_double_p, _c_double_p]),
     "hphc_set_kernel_timing": (ctypes.c_int, [_handle, ctypes.c_int]),
+    "hphc_set_sweep_shape": (ctypes.c_int, [_handle, ctypes.c_int, ctypes.c_int]),
+    "hphc_get_sweep_shape": (ctypes.c_int, [_handle, _c_int_p, _c_int_p]),
     "hphc_get_kernel_times": (ctypes.c_int, [_handle, ctypes.POINTER(ctypes.c_float),
                                              ctypes.POINTER(ctypes.c_float)]),
 }

@@ -19,6 +19,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <new>
 #include <numeric>
 #include <string>
@@ -146,6 +147,11 @@ cudaError_t ex2_fix_for_device(int device, cudaStream_t stream, float* fix, doub
     return cudaSuccess;
 }
 
+// Autotuned sweep shapes, per process: key (size bucket, D, precision,
+// variant) -> (events per thread, items per SM).
+std::mutex gTuneMutex;
+std::map<long, std::pair<int, int>> gTuneCache;
+
 }  // namespace
 
 struct hphc_engine {
@@ -177,10 +183,16 @@ struct hphc_engine {
     // scratch
     DevBuf<double> dPartials, dBlockSums, dOut, dProbs;
 
-    // plan
-    int R = 2;
+    // plan (sweep shape); fixedR / fixedItems = 0 lets the autotuner choose
+    int R = 2, itemsPerSM = 8;
+    int fixedR = 0, fixedItems = 0;
+    bool tuned = false;
     SweepGeometry geom{};
 
+    // FP32 variant (bit 0: coordinate lo parts, bit 1: software exponential)
+    int f32Variant = 1;
+    // scales the FP32 records were last packed with (-1: not packed)
+    double packedX = -1.0, packedT = -1.0;
     // FP32 exponential bias correction (see PairConsts::ex2Fix)
     float ex2Fix = 0.0f;
     double ex2Bias = 0.0;
@@ -208,18 +220,114 @@ struct hphc_engine {
                     "%s: %s", what, cudaGetErrorString(e));
     }
 
-    void plan() {
-        const int stripEvents = kSweepThreads * R;
-        geom.N = N;
-        geom.nTiles = (N + kTile - 1) / kTile;
-        geom.nStrips = (N + stripEvents - 1) / stripEvents;
-        geom.Npad = geom.nStrips * stripEvents;
-        // Enough (strip, chunk) CTAs for several waves on every SM.
-        const int target = numSMs * 8;
-        int nChunks = std::max(1, (target + geom.nStrips - 1) / geom.nStrips);
-        nChunks = std::min(nChunks, geom.nTiles);
-        geom.chunkTiles = (geom.nTiles + nChunks - 1) / nChunks;
-        geom.nChunks = (geom.nTiles + geom.chunkTiles - 1) / geom.chunkTiles;
+    // Geometry for R events per thread and `items` (strip, j-range) CTAs per
+    // SM (several waves, so the hardware scheduler balances uneven items).
+    SweepGeometry plan_for(int r, int items) const {
+        SweepGeometry g{};
+        const int stripEvents = kSweepThreads * r;
+        g.N = N;
+        g.nTiles = (N + kTile - 1) / kTile;
+        g.nStrips = (N + stripEvents - 1) / stripEvents;
+        g.Npad = g.nStrips * stripEvents;
+        const int target = numSMs * items;
+        int nChunks = std::max(1, (target + g.nStrips - 1) / g.nStrips);
+        nChunks = std::min(nChunks, g.nTiles);
+        g.chunkTiles = (g.nTiles + nChunks - 1) / nChunks;
+        g.nChunks = (g.nTiles + g.chunkTiles - 1) / g.chunkTiles;
+        return g;
+    }
+
+    int set_plan(int r, int items) {
+        const SweepGeometry g = plan_for(r, items);
+        cudaError_t e = dPartials.reserve((size_t)g.nChunks * kNumAcc * g.Npad);
+        if (e != cudaSuccess) return cuda_fail(e, "device allocation");
+        R = r;
+        itemsPerSM = items;
+        geom = g;
+        return HPHC_OK;
+    }
+
+    int launch_sweep(const PairConsts& c) {
+        cudaError_t e;
+        if (precision == HPHC_PRECISION_FP64)
+            e = launch_sweep_f64(D, R, geom, dRecF64.p, dTileMin.p, dTileMax.p, c, dPartials.p,
+                                 stream);
+        else
+            e = launch_sweep_f32c(D, R, f32Variant, geom, dRecF32.p, dTileMin.p, dTileMax.p, c,
+                                  dPartials.p, stream);
+        if (e != cudaSuccess) return cuda_fail(e, "sweep kernel");
+        return HPHC_OK;
+    }
+
+    // Autotuner: time every candidate shape on this engine's data (one warm
+    // and one timed sweep each), keep the fastest, cache it per process.
+    int autotune(const PairConsts& c) {
+        const long key = tune_key();
+        {
+            std::lock_guard<std::mutex> lock(gTuneMutex);
+            auto it = gTuneCache.find(key);
+            if (it != gTuneCache.end()) {
+                tuned = true;
+                return set_plan(fixedR ? fixedR : it->second.first,
+                                fixedItems ? fixedItems : it->second.second);
+            }
+        }
+        std::vector<int> rs, its;
+        if (fixedR) rs = {fixedR};
+        else if (precision == HPHC_PRECISION_FP64) rs = {1, 2};
+        else rs = {2, 4};
+        if (fixedItems) its = {fixedItems};
+        else its = {8, 16, 32, 64};
+        float best = 1e30f;
+        int bestR = rs[0], bestI = its[0];
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        int st = HPHC_OK;
+        for (int r : rs) {
+            for (int it : its) {
+                if ((st = set_plan(r, it))) break;
+                if ((st = launch_sweep(c))) break;  // warm
+                cudaEventRecord(e0, stream);
+                if ((st = launch_sweep(c))) break;
+                cudaEventRecord(e1, stream);
+                lastLaunches += 2;
+                cudaError_t err = cudaEventSynchronize(e1);
+                if (err != cudaSuccess) {
+                    st = cuda_fail(err, "autotune");
+                    break;
+                }
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (ms < best) {
+                    best = ms;
+                    bestR = r;
+                    bestI = it;
+                }
+            }
+            if (st) break;
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (st) return st;
+        {
+            std::lock_guard<std::mutex> lock(gTuneMutex);
+            gTuneCache[key] = {bestR, bestI};
+        }
+        tuned = true;
+        return set_plan(bestR, bestI);
+    }
+
+    long tune_key() const {
+        int lg = 0;
+        while ((1 << lg) < N) ++lg;  // power-of-two size bucket
+        return ((long)lg << 16) | ((long)D << 8) | ((long)precision << 4) | (long)f32Variant;
+    }
+
+    // Record scales of the FP32 path: x' = x sX, t' = t sT make the background
+    // exponent (log2 units) -(|dx'|^2 + dt'^2).
+    static double record_scale(double precisionParam) {
+        return std::fabs(precisionParam) * std::sqrt(0.5 * kLog2e);
     }
 
     PairConsts pair_consts(const double* p) const {
@@ -229,11 +337,12 @@ struct hphc_engine {
         c.cB = -0.5 * b * b;
         c.cS = -0.5 * sigma * sigma;
         c.cW = -omega;
-        split_float(c.cA * kLog2e, c.fAh, c.fAl);
-        split_float(c.cB * kLog2e, c.fBh, c.fBl);
-        split_float(c.cS * kLog2e, c.fSh, c.fSl);
-        split_float(c.cW * kLog2e, c.fWh, c.fWl);
-        c.ex2Fix = precision == HPHC_PRECISION_FP64 ? 0.0f : ex2Fix;
+        if (precision != HPHC_PRECISION_FP64) {
+            const double sT = record_scale(b);
+            split_float(-(sigma * sigma) / (a * a), c.fSh, c.fSl);
+            split_float(-omega * kLog2e / sT, c.fWh, c.fWl);
+        }
+        c.ex2Fix = (precision == HPHC_PRECISION_FP64 || (f32Variant & 2)) ? 0.0f : ex2Fix;
         const double thr = precision == HPHC_PRECISION_FP64 ? kSkipF64 : kSkipF32;
         c.skipB = (underflowSkip && c.cB < 0.0 && c.cA <= 0.0) ? thr : -1.0;
         c.skipS = (underflowSkip && c.cW < 0.0 && c.cS <= 0.0) ? thr : -1.0;
@@ -252,6 +361,13 @@ struct hphc_engine {
         f.seScale = f.omega * std::pow(f.sigma, D) * kInvSqrt2Pi;
         f.prefB = f.mu0 * f.bgScale;
         f.prefS = f.theta * f.seScale;
+        for (int q = 0; q < kNumAcc; ++q) f.accScale[q] = 1.0;
+        if (precision != HPHC_PRECISION_FP64) {
+            const double sX = record_scale(f.a), sT = record_scale(f.b);
+            f.accScale[1] = f.accScale[4] = 1.0 / (sX * sX);  // sums of d'^2
+            f.accScale[2] = 1.0 / (sT * sT);                  // sum of dt'^2
+            f.accScale[5] = 1.0 / sT;                         // sum of dt'
+        }
         f.T = hTimes.p[N - 1];
         // src/NewHawkes.hpp:659: locationCount * (embeddingDimension - 1) * log(M_1_SQRT_2PI)
         f.constant = (double)(N * (D - 1)) * std::log(kInvSqrt2Pi);
@@ -276,30 +392,49 @@ struct hphc_engine {
             if ((e = cudaMemcpyAsync(dRanks.p, hRanks.p, (size_t)N * sizeof(int32_t),
                                      cudaMemcpyHostToDevice, stream)) != cudaSuccess)
                 return cuda_fail(e, "upload ranks");
-            e = launch_pack_f32(D, N, dLoc.p, dTimes.p, dRanks.p, dRecF32.p, dTileMin.p,
-                                dTileMax.p, stream);
-            lastLaunches += 2;
+            e = launch_tile_bounds(N, dTimes.p, dTileMin.p, dTileMax.p, stream);
+            lastLaunches += 1;
+            packedX = packedT = -1.0;  // records must be rebuilt
         }
         if (e != cudaSuccess) return cuda_fail(e, "pack kernel");
         dirty = false;
         return HPHC_OK;
     }
 
+    // FP32 records are scaled by the current background precisions: rebuild
+    // them when those change.
+    int pack_f32_for(const double* p) {
+        if (!(p[1] != 0.0 && p[2] != 0.0 && std::isfinite(p[1]) && std::isfinite(p[2])))
+            return fail(HPHC_ERR_UNSUPPORTED,
+                        "FP32-compensated mode needs finite non-zero tauXprec and tauTprec "
+                        "(got %g, %g); use the FP64 mode", p[1], p[2]);
+        const double sX = record_scale(p[1]), sT = record_scale(p[2]);
+        if (sX == packedX && sT == packedT) return HPHC_OK;
+        cudaError_t e = launch_pack_f32(D, N, dLoc.p, dTimes.p, dRanks.p, sX, sT, dRecF32.p, stream);
+        if (e != cudaSuccess) return cuda_fail(e, "pack kernel");
+        lastLaunches += 1;
+        packedX = sX;
+        packedT = sT;
+        return HPHC_OK;
+    }
+
     // Enqueue sweep + finish + final for parameter vector p; results land in
     // dOut[slot*8 .. slot*8+7] (and dProbs if wantProbs).
     int enqueue_eval(const double* p, int slot, bool wantProbs) {
+        if (precision != HPHC_PRECISION_FP64) {
+            const int st = pack_f32_for(p);
+            if (st) return st;
+        }
         const PairConsts c = pair_consts(p);
         const FinishConsts f = finish_consts(p);
         lastConsts = c;
+        if (!tuned) {
+            const int st = autotune(c);
+            if (st) return st;
+        }
         cudaError_t e;
         if (kernelTiming) cudaEventRecord(evSweep0, stream);
-        if (precision == HPHC_PRECISION_FP64)
-            e = launch_sweep_f64(D, R, geom, dRecF64.p, dTileMin.p, dTileMax.p, c, dPartials.p,
-                                 stream);
-        else
-            e = launch_sweep_f32c(D, R, geom, dRecF32.p, dTileMin.p, dTileMax.p, c, dPartials.p,
-                                  stream);
-        if (e != cudaSuccess) return cuda_fail(e, "sweep kernel");
+        if (const int st = launch_sweep(c)) return st;
         if (kernelTiming) cudaEventRecord(evSweep1, stream);
         e = launch_finish(geom, dPartials.p, dTimes.p, f, dBlockSums.p,
                           wantProbs ? dProbs.p : nullptr, stream);
@@ -341,6 +476,7 @@ struct hphc_engine {
         precision = (fl & (HPHC_FLAG_FLOAT | HPHC_FLAG_COMPENSATED)) ? HPHC_PRECISION_FP32_COMP
                                                                       : HPHC_PRECISION_FP64;
         underflowSkip = !(fl & HPHC_FLAG_NO_UNDERFLOW_SKIP);
+        f32Variant = ((fl & HPHC_FLAG_FP32_SPACE_HILO) ? 1 : 0) | ((fl & HPHC_FLAG_FP32_FAST_EXP) ? 0 : 2);
         int count = 0;
         if (cudaGetDeviceCount(&count) != cudaSuccess || count < 1)
             return fail(HPHC_ERR_NO_DEVICE, "no CUDA device visible");
@@ -353,11 +489,10 @@ struct hphc_engine {
         if ((e = cudaEventCreate(&evSweep0)) || (e = cudaEventCreate(&evSweep1)) ||
             (e = cudaEventCreate(&evFinish1)))
             return cuda_fail(e, "create events");
-        if (precision != HPHC_PRECISION_FP64 &&
+        if (precision != HPHC_PRECISION_FP64 && !(f32Variant & 2) &&
             (e = ex2_fix_for_device(device, stream, &ex2Fix, &ex2Bias)) != cudaSuccess)
             return cuda_fail(e, "exponential calibration");
-        R = 2;
-        plan();
+        if (int st = set_plan(2, 8)) return st;
         const size_t nl = (size_t)N * D;
         if ((e = hLoc[0].reserve(nl)) || (e = hLoc[1].reserve(nl)) || (e = hTimes.reserve(N)) ||
             (e = hRanks.reserve(N)) || (e = hOut.reserve(8)))
@@ -368,7 +503,6 @@ struct hphc_engine {
         std::memset(hRanks.p, 0, (size_t)N * sizeof(int32_t));
         if ((e = dLoc.reserve(nl)) || (e = dTimes.reserve(N)) ||
             (e = dTileMin.reserve(geom.nTiles)) || (e = dTileMax.reserve(geom.nTiles)) ||
-            (e = dPartials.reserve((size_t)geom.nChunks * kNumAcc * geom.Npad)) ||
             (e = dBlockSums.reserve((size_t)finish_blocks(N) * 8)) || (e = dOut.reserve(8)) ||
             (e = dProbs.reserve(N)))
             return cuda_fail(e, "device allocation");
@@ -699,6 +833,34 @@ int hphc_get_last_launch_stats(hphc_engine* e, int* kernelLaunches, double* back
         if (backgroundTerms) *backgroundTerms = nb;
         if (selfExciteTerms) *selfExciteTerms = ns;
     }
+    return HPHC_OK;
+}
+
+int hphc_set_sweep_shape(hphc_engine* e, int eventsPerThread, int itemsPerSM) {
+    if (!e) return HPHC_ERR_INVALID_HANDLE;
+    const bool fp64 = e->precision == HPHC_PRECISION_FP64;
+    const bool okR = eventsPerThread == 0 ||
+                     (fp64 ? (eventsPerThread == 1 || eventsPerThread == 2)
+                           : (eventsPerThread == 2 || eventsPerThread == 4));
+    if (!okR) return e->fail(HPHC_ERR_BAD_ARGUMENT, "events per thread %d not supported",
+                             eventsPerThread);
+    if (itemsPerSM < 0 || itemsPerSM > 1024)
+        return e->fail(HPHC_ERR_BAD_ARGUMENT, "items per SM %d out of range", itemsPerSM);
+    e->fixedR = eventsPerThread;
+    e->fixedItems = itemsPerSM;
+    e->tuned = false;
+    if (eventsPerThread && itemsPerSM) {
+        DeviceGuard g(e->device);
+        e->tuned = true;
+        return e->set_plan(eventsPerThread, itemsPerSM);
+    }
+    return HPHC_OK;
+}
+
+int hphc_get_sweep_shape(hphc_engine* e, int* eventsPerThread, int* itemsPerSM) {
+    if (!e) return HPHC_ERR_INVALID_HANDLE;
+    if (eventsPerThread) *eventsPerThread = e->R;
+    if (itemsPerSM) *itemsPerSM = e->itemsPerSM;
     return HPHC_OK;
 }
 

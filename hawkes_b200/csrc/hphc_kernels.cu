@@ -25,7 +25,11 @@ namespace {
 
 constexpr double kInvSqrt2Pi = 0.398942280401432677939946059934;
 constexpr double kSqrtHalf = 0.707106781186547524400844362105;
-constexpr int kFlush = 32;  // FP32 partial sums are moved into FP64 every kFlush j events
+// FP32 partial sums are moved into FP64 every kFlush j events.  The FP32
+// accumulation error of a block grows like sqrt(kFlush) ulps; 32 keeps the
+// strongly cancelling gradient components (d/d tauX, d/d tauT) within 1e-8 of
+// their scale at N = 50,000, where 128 does not, for ~0.4 issue slots a pair.
+constexpr int kFlush = 32;
 
 __device__ __forceinline__ float ex2_ftz(float x) {
     float y;
@@ -52,19 +56,19 @@ __global__ void pack_f64_kernel(int N, const double* __restrict__ loc,
 template <int D>
 __global__ void pack_f32_kernel(int N, const double* __restrict__ loc,
                                 const double* __restrict__ times, const int32_t* __restrict__ ranks,
-                                float* __restrict__ rec) {
+                                double sX, double sT, float* __restrict__ rec) {
     constexpr int S = Layout<D>::kF32Stride;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
     float* r = rec + (size_t)i * S;
 #pragma unroll
     for (int k = 0; k < D; ++k) {
-        const double v = loc[(size_t)i * D + k];
+        const double v = loc[(size_t)i * D + k] * sX;
         const float h = (float)v;
         r[k] = h;
         r[D + 1 + k] = (float)(v - (double)h);
     }
-    const double v = times[i];
+    const double v = times[i] * sT;
     const float h = (float)v;
     r[D] = h;
     r[2 * D + 1] = (float)(v - (double)h);
@@ -238,15 +242,71 @@ sweep_f64_kernel(SweepGeometry g, const double* __restrict__ rec,
 
 // ------------------------------------------------ FP32-compensated sweep --
 //
-// Differences are formed from hi/lo float pairs, dd = (hi_i - hi_j) + (lo_i - lo_j),
-// so the FP32 representation error of the inputs (ulp(8760 h) ~ 1e-3 h) never
-// enters dt or d.  The exponent coefficients are split hi + lo as well, so
-// their FP32 rounding does not bias every term in the same direction.  The
-// six sums are kept in FP32 over kFlush consecutive j and then added to FP64
-// accumulators (blocked compensated summation); the cross-tile, cross-chunk
-// and per-event finish are FP64.
+// Records hold coordinates and times pre-scaled by the background kernel's
+// precisions, x' = x a sqrt(log2(e)/2) and t' = t b sqrt(log2(e)/2), so the
+// background exponent in log2 units is -(|dx'|^2 + dt'^2) with no coefficient
+// at all (hence no coefficient rounding).  Times are formed from hi/lo float
+// pairs, dt' = (hi_i - hi_j) + (lo_i - lo_j), so the FP32 representation error
+// of the inputs (ulp(8760 h) ~ 1e-3 h) never enters dt; coordinates likewise
+// when the variant keeps their lo parts.  The self-excitation exponent
+// kS |dx'|^2 + kW dt' uses hi + lo coefficients so their FP32 rounding does
+// not bias every term in the same direction.  The weighted sums come out in
+// scaled units and the finish rescales them in FP64.  The six sums are kept in FP32 over
+// kFlush consecutive j and then added to FP64 accumulators (blocked
+// compensated summation); the cross-tile, cross-chunk and per-event finish are
+// FP64.
+//
+// Variant bits (template parameter V):
+//   kSpaceLo  coordinate differences use the lo parts too (else hi only: the
+//             coordinate rounding then acts as a fixed ~1e-7 relative
+//             perturbation of each event's location, unbiased across events).
+//   kPolyExp  exponentials by exp2_poly (unbiased to ~3e-10) instead of
+//             ex2.approx with the measured mean-bias offset.
+constexpr int kSpaceLo = 1;
+constexpr int kPolyExp = 2;
 
-template <int D, int R, bool DO_B, bool DO_S, bool MASK>
+// Coefficients of p(f) ~ 2^f on [-1/2, 1/2], degree 7, fitted in relative
+// error by hawkes_b200/csrc/fit_exp2.py with sequential FP32 rounding; max
+// relative error 3.4e-10 with these FP32 values (FP64 evaluation).
+constexpr float kP1 = 0x1.62e43p-1f;
+constexpr float kP2 = 0x1.ebfbep-3f;
+constexpr float kP3 = 0x1.c6b07p-5f;
+constexpr float kP4 = 0x1.3b2a78p-7f;
+constexpr float kP5 = 0x1.5da248p-10f;
+constexpr float kP6 = 0x1.43ec02p-13f;
+constexpr float kP7 = 0x1.e50106p-17f;
+
+// 2^x for x <= 127 on the FMA pipe: Cody-Waite reduction x = n + f with
+// n = round(x) (added to 1.5 * 2^23 so the integer lands in the low mantissa
+// bits), |f| <= 1/2, p(f) by Horner, and 2^n built directly in the exponent
+// field: bits(t) << 23 == n << 23 (mod 2^32) because the magic constant's bits
+// all shift out.  Arguments below -126.5 give n = -127 and a scale of exactly
+// +0, so the result is +0 as with ex2.approx.ftz and the tile-level underflow
+// skip stays exact.
+__device__ __forceinline__ float exp2_poly(float x) {
+    x = fmaxf(x, -127.0f);
+    const float t = x + 12582912.0f;
+    const float n = t - 12582912.0f;
+    const float f = x - n;
+    float p = kP7;
+    p = fmaf(p, f, kP6);
+    p = fmaf(p, f, kP5);
+    p = fmaf(p, f, kP4);
+    p = fmaf(p, f, kP3);
+    p = fmaf(p, f, kP2);
+    p = fmaf(p, f, kP1);
+    p = fmaf(p, f, 1.0f);
+    const float s = __uint_as_float((__float_as_uint(t) << 23) + 0x3F800000u);
+    return p * s;
+}
+
+template <int V>
+__device__ __forceinline__ float exp2_term(float e) {
+    if (V & kPolyExp) return exp2_poly(e);
+    return ex2_ftz(e);
+}
+
+template <int D, int R, int V, bool DO_B, bool DO_S, bool MASK>
 __device__ __forceinline__ void body_f32(const float* __restrict__ sRec, int jb, int je,
                                          const float (&xh)[R][D], const float (&xl)[R][D],
                                          const float (&th)[R], const float (&tl)[R],
@@ -269,23 +329,24 @@ __device__ __forceinline__ void body_f32(const float* __restrict__ sRec, int jb,
             float d2 = 0.0f;
 #pragma unroll
             for (int k = 0; k < D; ++k) {
-                const float dd = (xh[r][k] - rj[k]) + (xl[r][k] - rj[D + 1 + k]);
+                const float dd = (V & kSpaceLo) ? (xh[r][k] - rj[k]) + (xl[r][k] - rj[D + 1 + k])
+                                                : xh[r][k] - rj[k];
                 d2 = fmaf(dd, dd, d2);
             }
             const float dt = (th[r] - rj[D]) + (tl[r] - rj[2 * D + 1]);
             if (DO_B) {
                 const float t2 = dt * dt;
-                const float e =
-                    fmaf(c.fAh, d2, fmaf(c.fBh, t2, fmaf(c.fAl, d2, fmaf(c.fBl, t2, c.ex2Fix))));
-                const float B = ex2_ftz(e);
+                const float e = (V & kPolyExp) ? -(d2 + t2) : (c.ex2Fix - d2) - t2;
+                const float B = exp2_term<V>(e);
                 a[r][0] += B;
                 a[r][1] = fmaf(B, d2, a[r][1]);
                 a[r][2] = fmaf(B, t2, a[r][2]);
             }
             if (DO_S) {
-                const float e =
-                    fmaf(c.fSh, d2, fmaf(c.fWh, dt, fmaf(c.fSl, d2, fmaf(c.fWl, dt, c.ex2Fix))));
-                float Sv = ex2_ftz(e);
+                const float e = fminf(
+                    fmaf(c.fSh, d2, fmaf(c.fWh, dt, fmaf(c.fSl, d2, fmaf(c.fWl, dt, c.ex2Fix)))),
+                    127.0f);
+                float Sv = exp2_term<V>(e);
                 if (MASK) Sv = rk[r] > __float_as_int(rj[2 * D + 2]) ? Sv : 0.0f;
                 a[r][3] += Sv;
                 a[r][4] = fmaf(Sv, d2, a[r][4]);
@@ -295,7 +356,7 @@ __device__ __forceinline__ void body_f32(const float* __restrict__ sRec, int jb,
     }
 }
 
-template <int D, int R, bool DO_B, bool DO_S, bool MASK>
+template <int D, int R, int V, bool DO_B, bool DO_S, bool MASK>
 __device__ __forceinline__ void tile_f32(const float* __restrict__ sRec, int nj,
                                          const float (&xh)[R][D], const float (&xl)[R][D],
                                          const float (&th)[R], const float (&tl)[R],
@@ -307,7 +368,8 @@ __device__ __forceinline__ void tile_f32(const float* __restrict__ sRec, int nj,
         for (int r = 0; r < R; ++r)
 #pragma unroll
             for (int q = 0; q < kNumAcc; ++q) a[r][q] = 0.0f;
-        body_f32<D, R, DO_B, DO_S, MASK>(sRec, jb, min(jb + kFlush, nj), xh, xl, th, tl, rk, c, a);
+        body_f32<D, R, V, DO_B, DO_S, MASK>(sRec, jb, min(jb + kFlush, nj), xh, xl, th, tl, rk, c,
+                                            a);
 #pragma unroll
         for (int r = 0; r < R; ++r)
 #pragma unroll
@@ -315,7 +377,7 @@ __device__ __forceinline__ void tile_f32(const float* __restrict__ sRec, int nj,
     }
 }
 
-template <int D, int R>
+template <int D, int R, int V>
 __global__ void __launch_bounds__(kSweepThreads)
 sweep_f32c_kernel(SweepGeometry g, const float* __restrict__ rec,
                   const double* __restrict__ tileMin, const double* __restrict__ tileMax,
@@ -371,16 +433,16 @@ sweep_f32c_kernel(SweepGeometry g, const float* __restrict__ rec,
         __syncthreads();
         if (m.doB) {
             if (!m.doS)
-                tile_f32<D, R, true, false, false>(sRec, nj, xh, xl, th, tl, rk, c, acc);
+                tile_f32<D, R, V, true, false, false>(sRec, nj, xh, xl, th, tl, rk, c, acc);
             else if (m.allCausal)
-                tile_f32<D, R, true, true, false>(sRec, nj, xh, xl, th, tl, rk, c, acc);
+                tile_f32<D, R, V, true, true, false>(sRec, nj, xh, xl, th, tl, rk, c, acc);
             else
-                tile_f32<D, R, true, true, true>(sRec, nj, xh, xl, th, tl, rk, c, acc);
+                tile_f32<D, R, V, true, true, true>(sRec, nj, xh, xl, th, tl, rk, c, acc);
         } else {
             if (m.allCausal)
-                tile_f32<D, R, false, true, false>(sRec, nj, xh, xl, th, tl, rk, c, acc);
+                tile_f32<D, R, V, false, true, false>(sRec, nj, xh, xl, th, tl, rk, c, acc);
             else
-                tile_f32<D, R, false, true, true>(sRec, nj, xh, xl, th, tl, rk, c, acc);
+                tile_f32<D, R, V, false, true, true>(sRec, nj, xh, xl, th, tl, rk, c, acc);
         }
     }
 #pragma unroll
@@ -436,7 +498,7 @@ finish_kernel(SweepGeometry g, const double* __restrict__ partials,
             double acc = 0.0;
             for (int ch = 0; ch < g.nChunks; ++ch)
                 acc += partials[((size_t)ch * kNumAcc + q) * g.Npad + i];
-            s[q] = acc;
+            s[q] = acc * f.accScale[q];
         }
         const double SB = f.prefB * s[0];
         const double SS = f.prefS * s[3];
@@ -519,16 +581,21 @@ cudaError_t launch_pack_f64(int D, int N, const double* loc, const double* times
 }
 
 cudaError_t launch_pack_f32(int D, int N, const double* loc, const double* times,
-                            const int32_t* ranks, float* rec, double* tileMin, double* tileMax,
+                            const int32_t* ranks, double sX, double sT, float* rec,
                             cudaStream_t s) {
     const int blocks = (N + 255) / 256;
     switch (D) {
 #define X(d) \
-    case d: pack_f32_kernel<d><<<blocks, 256, 0, s>>>(N, loc, times, ranks, rec); break;
+    case d: pack_f32_kernel<d><<<blocks, 256, 0, s>>>(N, loc, times, ranks, sX, sT, rec); break;
         HPHC_FOR_EACH_DIM(X)
 #undef X
         default: return cudaErrorInvalidValue;
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_tile_bounds(int N, const double* times, double* tileMin, double* tileMax,
+                               cudaStream_t s) {
     tile_bounds_kernel<<<(N + kTile - 1) / kTile, kTile, 0, s>>>(N, times, tileMin, tileMax);
     return cudaGetLastError();
 }
@@ -556,27 +623,36 @@ cudaError_t launch_sweep_f64(int D, int R, const SweepGeometry& g, const double*
     return cudaGetLastError();
 }
 
-cudaError_t launch_sweep_f32c(int D, int R, const SweepGeometry& g, const float* rec,
+template <int D, int R>
+static cudaError_t launch_f32c_variant(int V, int grid, const SweepGeometry& g, const float* rec,
+                                       const double* tileMin, const double* tileMax,
+                                       const PairConsts& c, double* partials, cudaStream_t s) {
+    switch (V) {
+        case 0: sweep_f32c_kernel<D, R, 0><<<grid, kSweepThreads, 0, s>>>(g, rec, tileMin, tileMax, c, partials); break;
+        case 1: sweep_f32c_kernel<D, R, 1><<<grid, kSweepThreads, 0, s>>>(g, rec, tileMin, tileMax, c, partials); break;
+        case 2: sweep_f32c_kernel<D, R, 2><<<grid, kSweepThreads, 0, s>>>(g, rec, tileMin, tileMax, c, partials); break;
+        case 3: sweep_f32c_kernel<D, R, 3><<<grid, kSweepThreads, 0, s>>>(g, rec, tileMin, tileMax, c, partials); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sweep_f32c(int D, int R, int V, const SweepGeometry& g, const float* rec,
                               const double* tileMin, const double* tileMax, const PairConsts& c,
                               double* partials, cudaStream_t s) {
     const int grid = g.nStrips * g.nChunks;
-#define X(d)                                                                                     \
-    case d:                                                                                      \
-        if (R == 2)                                                                              \
-            sweep_f32c_kernel<d, 2><<<grid, kSweepThreads, 0, s>>>(g, rec, tileMin, tileMax, c,  \
-                                                                    partials);                   \
-        else if (R == 4)                                                                         \
-            sweep_f32c_kernel<d, 4><<<grid, kSweepThreads, 0, s>>>(g, rec, tileMin, tileMax, c,  \
-                                                                    partials);                   \
-        else                                                                                     \
-            return cudaErrorInvalidValue;                                                        \
-        break;
+#define X(d)                                                                                    \
+    case d:                                                                                     \
+        if (R == 2) return launch_f32c_variant<d, 2>(V, grid, g, rec, tileMin, tileMax, c,      \
+                                                     partials, s);                              \
+        if (R == 4) return launch_f32c_variant<d, 4>(V, grid, g, rec, tileMin, tileMax, c,      \
+                                                     partials, s);                              \
+        return cudaErrorInvalidValue;
     switch (D) {
         HPHC_FOR_EACH_DIM(X)
         default: return cudaErrorInvalidValue;
     }
 #undef X
-    return cudaGetLastError();
 }
 
 cudaError_t launch_finish(const SweepGeometry& g, const double* partials, const double* times,

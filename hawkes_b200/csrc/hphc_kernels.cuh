@@ -39,8 +39,10 @@ struct Layout {
 // with cA = -a^2/2, cB = -b^2/2, cS = -sigma^2/2, cW = -omega.
 struct PairConsts {
     double cA, cB, cS, cW;                 // natural-log units (FP64 path)
-    float fAh, fAl, fBh, fBl;              // log2-unit coefficients split hi + lo
-    float fSh, fSl, fWh, fWl;              //   (FP32 path): f = cX*log2(e) = fXh + fXl
+    // FP32 path, on records scaled by sX = |a| sqrt(log2(e)/2), sT = |b| sqrt(log2(e)/2):
+    // S exponent (log2 units) = kS |dx'|^2 + kW dt' with kS = -sigma^2 / a^2 and
+    // kW = -omega log2(e) / sT, each split hi + lo.
+    float fSh, fSl, fWh, fWl;
     // Added to every FP32 exponent: -log2(1 + beta), where beta is the mean
     // relative error of ex2.approx.ftz.f32 measured on the device at engine
     // creation (the instruction rounds low on average), so the FP32 pair
@@ -59,6 +61,7 @@ struct FinishConsts {
     double prefS;     // theta omega sigma^D / sqrt(2 pi) : S_ij = prefS * S_u
     double bgScale;   // prefB / mu0
     double seScale;   // prefS / theta
+    double accScale[6];  // multiplies the six unit pair sums (undoes the record scaling)
     double T;         // t[N-1]
     double constant;  // N (D-1) log(1/sqrt(2 pi))
     int D;
@@ -79,16 +82,22 @@ struct SweepGeometry {
 // compute per-tile time bounds.  ranks may be null for the FP64 layout.
 cudaError_t launch_pack_f64(int D, int N, const double* loc, const double* times, double* rec,
                             double* tileMin, double* tileMax, cudaStream_t s);
+// FP32 records of coordinates scaled by sX and times scaled by sT (no tile
+// bounds: those come from launch_tile_bounds).
 cudaError_t launch_pack_f32(int D, int N, const double* loc, const double* times,
-                            const int32_t* ranks, float* rec, double* tileMin, double* tileMax,
+                            const int32_t* ranks, double sX, double sT, float* rec,
                             cudaStream_t s);
+cudaError_t launch_tile_bounds(int N, const double* times, double* tileMin, double* tileMax,
+                               cudaStream_t s);
 
 // Pair sweep: fills partials[chunk][6][Npad] with unit pair sums.  R is the
 // number of target events per thread (strip = kSweepThreads * R events).
 cudaError_t launch_sweep_f64(int D, int R, const SweepGeometry& g, const double* rec,
                              const double* tileMin, const double* tileMax, const PairConsts& c,
                              double* partials, cudaStream_t s);
-cudaError_t launch_sweep_f32c(int D, int R, const SweepGeometry& g, const float* rec,
+// V selects the FP32 variant: bit 0 = coordinate lo parts, bit 1 = software
+// exponential (see hphc_kernels.cu).
+cudaError_t launch_sweep_f32c(int D, int R, int V, const SweepGeometry& g, const float* rec,
                               const double* tileMin, const double* tileMax, const PairConsts& c,
                               double* partials, cudaStream_t s);
 

@@ -44,6 +44,8 @@ AVX512 = 1 << 7
 CUDA = 1 << 8
 COMPENSATED = 1 << 9
 NO_UNDERFLOW_SKIP = 1 << 10
+FP32_FAST_EXP = 1 << 11
+FP32_SPACE_HILO = 1 << 12
 
 PRECISION_FP64 = 0
 PRECISION_FP32_COMP = 1
@@ -196,6 +198,18 @@ class CudaHawkes:
         self._check(_lib.hphc_read_results(self._h, ctypes.byref(ll), g.ctypes.data_as(_dp), 6),
                     "readResults")
         return ll.value, g
+
+    def setSweepShape(self, eventsPerThread: int = 0, itemsPerSM: int = 0) -> None:
+        """Fix the sweep shape (0 = autotune that dimension)."""
+        self._check(_lib.hphc_set_sweep_shape(self._h, int(eventsPerThread), int(itemsPerSM)),
+                    "setSweepShape")
+
+    def sweepShape(self):
+        r = ctypes.c_int()
+        i = ctypes.c_int()
+        self._check(_lib.hphc_get_sweep_shape(self._h, ctypes.byref(r), ctypes.byref(i)),
+                    "sweepShape")
+        return r.value, i.value
 
     def setKernelTiming(self, enable: bool = True) -> None:
         self._check(_lib.hphc_set_kernel_timing(self._h, int(bool(enable))), "setKernelTiming")

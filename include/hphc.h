@@ -60,6 +60,15 @@ extern "C" {
 #define HPHC_FLAG_COMPENSATED (1L << 9) /* new: FP32 pair terms, compensated, FP64 reductions */
 #define HPHC_FLAG_NO_UNDERFLOW_SKIP (1L << 10) /* new: evaluate every tile pair, even those
                                                   whose terms all underflow to zero */
+/* FP32-compensated mode only.  By default its exponentials are computed on the
+ * FMA pipe (range reduction + polynomial, unbiased to ~3e-10) and coordinate
+ * differences from FP32 coordinates (times always from hi/lo float pairs). */
+#define HPHC_FLAG_FP32_FAST_EXP (1L << 11)   /* hardware ex2.approx with its mean bias
+                                                (measured on the device) removed: ~1.6x
+                                                faster; strongly cancelling gradient
+                                                components lose accuracy (~1e-6) */
+#define HPHC_FLAG_FP32_SPACE_HILO (1L << 12) /* coordinate differences from hi/lo float
+                                                pairs (times always use hi/lo pairs) */
 
 /* Precision modes reported by hphc_get_precision(). */
 #define HPHC_PRECISION_FP64 0          /* plain FP64 pair terms and reductions           */
@@ -181,6 +190,14 @@ int hphc_read_results(hphc_engine* engine, double* loglik, double* gradient, siz
  * terms all underflow to exactly zero in the working precision. */
 int hphc_get_last_launch_stats(hphc_engine* engine, int* kernelLaunches,
                                double* backgroundTerms, double* selfExciteTerms);
+
+/* Sweep shape: target events per thread (2 or 4; a CTA strip holds 128 times
+ * as many) and the number of (strip, j-range) work items per SM the j range is
+ * split into.  0 for either lets the engine's autotuner choose it (timed on the
+ * engine's own data at the first evaluation, cached per process by problem
+ * size and mode). */
+int hphc_set_sweep_shape(hphc_engine* engine, int eventsPerThread, int itemsPerSM);
+int hphc_get_sweep_shape(hphc_engine* engine, int* eventsPerThread, int* itemsPerSM);
 
 /* Record CUDA events around the pair-sweep kernel and around the finish
  * kernels of every later evaluation (enable != 0), on the engine's stream. */

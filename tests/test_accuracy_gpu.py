@@ -66,6 +66,18 @@ def test_fp32_compensated_meets_1e8(c2):
     ll, g, probs = run(loc, t, p, hb.CUDA | hb.COMPENSATED)
     rel, gs, pe = report("fp32c", ll, g, probs, o)
     assert rel <= 1e-8
+    assert np.all(gs <= 1e-8)
+    assert pe <= 1e-5
+
+
+def test_fp32_fast_exp_meets_1e8_on_loglik(c2):
+    # Hardware ex2 with its mean bias removed: the log-likelihood and the
+    # gradient against its term-level (condition) scale meet 1e-8; strongly
+    # cancelling components (d/d tauX, d/d tauT) do not on the per-event scale.
+    loc, t, p, o = c2
+    ll, g, probs = run(loc, t, p, hb.CUDA | hb.COMPENSATED | hb.FP32_FAST_EXP)
+    rel, gs, pe = report("fp32c fast exp", ll, g, probs, o)
+    assert rel <= 1e-8
     assert np.all(np.abs(g - o["grad"]) <= 1e-8 * o["grad_term_scale"])
     assert pe <= 1e-5
 
