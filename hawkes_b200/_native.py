@@ -42,6 +42,9 @@ SIGNATURES = {
     "hphc_enqueue_log_likelihood_and_gradient": (ctypes.c_int, [_handle]),
     "hphc_read_results": (ctypes.c_int, [_handle, _c_double_p, _c_double_p, ctypes.c_size_t]),
     "hphc_get_last_launch_stats": (ctypes.c_int, [_handle, _c_int_p, _c_double_p, _c_double_p]),
+    "hphc_loglik_grad_fp64_static": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                                    ctypes.c_void_p, _c_double_p,
+                                                    ctypes.c_void_p, ctypes.c_void_p]),
     "hphc_set_kernel_timing": (ctypes.c_int, [_handle, ctypes.c_int]),
     "hphc_set_sweep_shape": (ctypes.c_int, [_handle, ctypes.c_int, ctypes.c_int]),
     "hphc_get_sweep_shape": (ctypes.c_int, [_handle, _c_int_p, _c_int_p]),

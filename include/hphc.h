@@ -165,6 +165,33 @@ int hphc_get_internal_dimension(hphc_engine* engine, int* out);
 int hphc_batch_log_likelihood_and_gradient(hphc_engine* engine, const double* params, int K,
                                            double* loglik, double* gradient);
 
+/* ---- evaluation without allocation (no reference counterpart) -----------
+ *
+ * FP64 log-likelihood and gradient of one event set for callers that must not
+ * allocate GPU memory while they run: code inside a framework that owns all
+ * device memory through its own pool or memory cap, real-time loops that
+ * cannot take an allocation's implicit synchronisation, processes with a GPU
+ * memory budget fixed at start-up.  This function calls no cudaMalloc,
+ * cudaFree or other allocating routine; all of its scratch is one 16 MiB
+ * static device array inside libhawkes_b200.so (held on every GPU that loads
+ * the library, until the process exits), enough for N up to about 200,000
+ * events at D = 2 (fewer at higher D).  Larger problems return
+ * HPHC_ERR_SCRATCH_TOO_SMALL without touching the GPU.
+ *
+ * Inputs are device memory of the current CUDA device: deviceLocations (N x D
+ * row-major), deviceTimes (N); params are 6 host doubles in reference order.
+ * deviceOut is 8 doubles of device memory: [0] log-likelihood, [1..6]
+ * gradient, [7] zero.  The call runs on `stream` (a cudaStream_t, or null
+ * for the default stream) and returns when the result is written.
+ *
+ * The first call on a device looks up the static array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * Every call shares the one array: calls that overlap on the GPU (other
+ * streams or threads) race and corrupt each other's results. */
+int hphc_loglik_grad_fp64_static(int embeddingDimension, int locationCount,
+                                 const double* deviceLocations, const double* deviceTimes,
+                                 const double* params, double* deviceOut, void* stream);
+
 /* ---- introspection and device-resident timing --------------------------- */
 
 /* Precision mode in use (HPHC_PRECISION_*). */
