@@ -228,55 +228,133 @@ def cpu_baseline(budget_s=15.0):
 
 # ------------------------------------------------------------------ our arm --
 
-def time_device(eng, steps, warmup, torch, stream, flush):
-    """Per-step device time (CUDA events on the engine's stream), L2 flushed
-    before each step outside the event pair; also the sweep-kernel time."""
-    eng.setKernelTiming(True)
+class Runner:
+    """One workload on one GPU: the timed step through the engine (data on the
+    device, CUDA-event step time recorded by the engine on its stream) and the
+    end-to-end step through the public API with host buffers."""
+
+    def __init__(self, hb, workload, flags, device):
+        self.hb, self.w, self.flags, self.device = hb, workload, flags, device
+        kind = workload["kind"]
+        if kind == "single":
+            loc, t, p = workload["loc"], workload["t"], workload["params"]
+            self.eng = hb.CudaHawkes(loc.shape[1], len(t), flags, device)
+            self.eng.setTimesData(t)
+            self.eng.updateLocations(-1, loc)
+            self.eng.setParameters(p)
+        elif kind == "batch":
+            loc, t = workload["loc"], workload["t"]
+            self.eng = hb.CudaHawkes(loc.shape[1], len(t), flags, device)
+            self.eng.setTimesData(t)
+            self.eng.updateLocations(-1, loc)
+        else:
+            sets = workload["sets"]
+            self.eng = hb.Multiset(2, [len(t) for _, t, _ in sets], flags, device)
+            for k, (loc, t, _) in enumerate(sets):
+                self.eng.setData(k, loc, t)
+        self.stream = (self.eng.stream if kind != "sets" else None)
+
+    def evaluate(self):
+        kind = self.w["kind"]
+        if kind == "single":
+            self.eng.enqueueLogLikelihoodAndGradient()
+            return self.eng.readResults()
+        if kind == "batch":
+            return self.eng.batchLogLikelihoodAndGradient(self.w["params"])
+        return self.eng.logLikelihoodAndGradient(self.w["params"])
+
+    def e2e_step(self):
+        kind, w = self.w["kind"], self.w
+        if kind == "single":
+            self.eng.setTimesData(w["t"])
+            self.eng.updateLocations(-1, w["loc"])
+            self.eng.setParameters(w["params"])
+            return self.eng.getLogLikelihoodAndGradient()
+        if kind == "batch":
+            self.eng.setTimesData(w["t"])
+            self.eng.updateLocations(-1, w["loc"])
+            return self.eng.batchLogLikelihoodAndGradient(w["params"])
+        for k, (loc, t, _) in enumerate(w["sets"]):
+            self.eng.setData(k, loc, t)
+        return self.eng.logLikelihoodAndGradient(w["params"])
+
+    def close(self):
+        self.eng.close()
+
+
+def time_device(run, steps, warmup, flush_fn):
+    """Per-step device time from the CUDA events the engine records on its own
+    stream around the step (table upload, record build, sweep, finish, result
+    copy); L2 is flushed before each step, outside those events.  Also the
+    sweep kernel's own event time."""
+    run.eng.setKernelTiming(True)
     for _ in range(warmup):
-        eng.enqueueLogLikelihoodAndGradient()
-        eng.readResults()
-    step_ms, sweep_ms = [], []
-    res = None
+        run.evaluate()
+    step_ms, sweep_ms, res = [], [], None
     for _ in range(steps):
-        with torch.cuda.stream(stream):
-            flush.zero_()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        eng.enqueueLogLikelihoodAndGradient()
-        e1.record(stream)
-        res = eng.readResults()
-        step_ms.append(e0.elapsed_time(e1))
-        sweep_ms.append(eng.kernelTimes()[0])
-    eng.setKernelTiming(False)
+        flush_fn()
+        res = run.evaluate()
+        sweep, _, step = run.eng.kernelTimes()
+        step_ms.append(step)
+        sweep_ms.append(sweep)
+    run.eng.setKernelTiming(False)
     return step_ms, sweep_ms, res
 
 
-def time_e2e(hb, flags, loc, t, p, steps, warmup, device):
-    eng = hb.CudaHawkes(2, len(t), flags, device)
-    loc_flat = np.ascontiguousarray(loc).reshape(-1)
-
-    def step():
-        eng.setTimesData(t)
-        eng.updateLocations(-1, loc_flat)
-        eng.setParameters(p)
-        return eng.getLogLikelihoodAndGradient()
-
+def time_e2e(run, steps, warmup):
     for _ in range(warmup):
-        step()
+        run.e2e_step()
     t0 = time.perf_counter()
     for _ in range(steps):
-        step()
-    dt = (time.perf_counter() - t0) / steps
-    eng.close()
-    return dt
+        run.e2e_step()
+    return (time.perf_counter() - t0) / steps
+
+
+def make_workload(name, n):
+    """The timed workloads; every other configuration is a parity-test case."""
+    from hawkes_b200 import workloads
+    base = workloads.BASE_PARAMS.copy()
+    if name == "headline":
+        loc, t = workloads.uniform(n, seed=SEED)
+        return {"kind": "single", "loc": loc, "t": t, "params": base, "pairs": float(n) * n,
+                "h2d": n * 2 * 8 + n * 8, "d2h": 64,
+                "desc": f"uniform N={n} D=2, 20x20 km, [0,8760) h sorted, seed {SEED}, base "
+                        "params; log-likelihood + 6-parameter gradient",
+                "config": {"N": n, "D": 2}}
+    if name == "batched":
+        loc, t = workloads.uniform(20000, seed=2)
+        P = workloads.proposals(256, seed=2)
+        return {"kind": "batch", "loc": loc, "t": t, "params": P, "pairs": 256 * 20000.0 ** 2,
+                "h2d": 20000 * 24 + P.size * 8, "d2h": 256 * 7 * 8,
+                "desc": "uniform N=20000 D=2 (seed 2), 256 proposals base*exp(0.3 z) (seed 2), "
+                        "one run; log-likelihood + gradient each",
+                "config": {"N": 20000, "K": 256, "D": 2}}
+    if name == "uneven":
+        sets = workloads.uneven(64, seed=3)
+        params = np.stack([p for _, _, p in sets])
+        sizes = [len(t) for _, t, _ in sets]
+        return {"kind": "sets", "sets": sets, "params": params,
+                "pairs": float(sum(float(m) * m for m in sizes)),
+                "h2d": sum(m * 24 for m in sizes) + params.size * 8, "d2h": 64 * 7 * 8,
+                "desc": "64 uniform sets, sizes log-uniform in [1e3, 1e5] (seed 3), own "
+                        "log-normal params each, one run; log-likelihood + gradient each",
+                "config": {"sets": 64, "N_total": int(sum(sizes)), "N_max": int(max(sizes)),
+                           "D": 2}}
+    if name == "clustered":
+        loc, t = workloads.clustered()
+        m = len(t)
+        return {"kind": "single", "loc": loc, "t": t, "params": base, "pairs": float(m) * m,
+                "h2d": m * 24, "d2h": 64,
+                "desc": "Hawkes branching process N=500000 (50x50 km, [0,8760) h, Poisson(0.5) "
+                        "offspring, seed 4), base params; log-likelihood + gradient",
+                "config": {"N": m, "D": 2}}
+    raise ValueError(name)
 
 
 def ours_arm(args):
     import torch
 
     import hawkes_b200 as hb
-    from hawkes_b200 import workloads
 
     rank, world, local = env_int("RANK", 0), env_int("WORLD_SIZE", 1), env_int("LOCAL_RANK", 0)
     torch.cuda.set_device(local)
@@ -288,22 +366,8 @@ def ours_arm(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
 
-    N = args.n
-    loc, t = workloads.uniform(N, seed=SEED)
-    p = workloads.BASE_PARAMS.copy()
+    w = make_workload(args.workload, args.n)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{local}")
-
-    def make(flags):
-        e = hb.CudaHawkes(2, N, flags, local)
-        e.setTimesData(t)
-        e.updateLocations(-1, loc)
-        e.setParameters(p)
-        return e
-
-    fp32 = make(hb.CUDA | hb.COMPENSATED)
-    fp64 = make(hb.CUDA)
-    s32 = torch.cuda.ExternalStream(fp32.stream, device=f"cuda:{local}")
-    s64 = torch.cuda.ExternalStream(fp64.stream, device=f"cuda:{local}")
 
     def barrier():
         torch.cuda.synchronize()
@@ -311,28 +375,46 @@ def ours_arm(args):
             dist.barrier()
         torch.cuda.synchronize()
 
+    def flusher(run):
+        if run.stream:
+            ext = torch.cuda.ExternalStream(run.stream, device=f"cuda:{local}")
+            def f():
+                with torch.cuda.stream(ext):
+                    flush.zero_()
+        else:
+            def f():
+                flush.zero_()
+                torch.cuda.synchronize()
+        return f
+
+    fp32 = Runner(hb, w, hb.CUDA | hb.COMPENSATED, local)
+    fp64 = Runner(hb, w, hb.CUDA, local)
+
     # FP64 plain path (the comparison in the metric)
     barrier()
-    ms64, sweep64, res64 = time_device(fp64, args.steps, args.warmup, torch, s64, flush)
+    ms64, sweep64, res64 = time_device(fp64, args.steps64 or args.steps, args.warmup,
+                                       flusher(fp64))
     barrier()
     # FP32-compensated path (the headline), clocks sampled while it runs
     with ClockSampler() as clocks:
         barrier()
-        ms32, sweep32, res32 = time_device(fp32, args.steps, args.warmup, torch, s32, flush)
+        ms32, sweep32, res32 = time_device(fp32, args.steps, args.warmup, flusher(fp32))
         barrier()
-    launches, nb, ns = fp32.lastLaunchStats()
-    shape32 = fp32.sweepShape()
-    _, nb64, ns64 = fp64.lastLaunchStats()
+    launches, nb, ns = fp32.eng.lastLaunchStats()
+    shape32 = fp32.eng.sweepShape() if w["kind"] != "sets" else None
+    _, nb64, ns64 = fp64.eng.lastLaunchStats()
+    steps64 = args.steps64 or args.steps
 
-    tot32 = torch.tensor([sum(ms32), sum(ms64)], dtype=torch.float64, device=f"cuda:{local}")
+    tot = torch.tensor([sum(ms32) / args.steps, sum(ms64) / steps64], dtype=torch.float64,
+                       device=f"cuda:{local}")
     if dist:
-        dist.all_reduce(tot32, op=dist.ReduceOp.MAX)
-    ms_step32 = float(tot32[0]) / args.steps
-    ms_step64 = float(tot32[1]) / args.steps
+        dist.all_reduce(tot, op=dist.ReduceOp.MAX)
+    ms_step32, ms_step64 = float(tot[0]), float(tot[1])
 
     # End to end through the public API with host buffers.
+    fp64.close()
     barrier()
-    e2e_s = time_e2e(hb, hb.CUDA | hb.COMPENSATED, loc, t, p, args.steps, args.warmup, local)
+    e2e_s = time_e2e(fp32, max(1, min(args.steps, 50)), args.warmup)
     e2e_t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local}")
     if dist:
         dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
@@ -340,14 +422,13 @@ def ours_arm(args):
 
     clock_summary = clocks.summary(None)
     fp32.close()
-    fp64.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     if rank != 0:
         return 0
 
-    pairs = float(N) * N
+    pairs = w["pairs"]
     value = world * pairs / (ms_step32 / 1e3)
     value64 = world * pairs / (ms_step64 / 1e3)
     peaks, peak_src = measured_peaks()
@@ -360,24 +441,31 @@ def ours_arm(args):
     tpath = os.path.join(ROOT, "profiles", "sweep_traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
-            traffic = json.load(f).get("fp32c_N100000_bytes_per_launch")
+            traffic = json.load(f).get(f"fp32c_{args.workload}_bytes_per_launch")
 
-    ll32, g32 = res32
-    ll64, g64 = res64
-    acc = {"loglik_rel_vs_fp64": abs(ll32 - ll64) / abs(ll64),
-           "grad_rel_vs_fp64": [abs(a - b) / abs(b) if b else None for a, b in zip(g32, g64)]}
+    ll32 = np.atleast_1d(np.asarray(res32[0], dtype=np.float64))
+    ll64 = np.atleast_1d(np.asarray(res64[0], dtype=np.float64))
+    g32 = np.atleast_2d(np.asarray(res32[1], dtype=np.float64))
+    g64 = np.atleast_2d(np.asarray(res64[1], dtype=np.float64))
+    acc = {"loglik_rel_vs_fp64_max": float(np.max(np.abs(ll32 - ll64) / np.abs(ll64))),
+           "grad_rel_vs_fp64_max": [float(v) for v in
+                                    np.max(np.abs(g32 - g64) / np.maximum(np.abs(g64), 1e-300),
+                                           axis=0)]}
+    kernel = ("sweep_f32c_list_kernel" +
+              (f"<D=2, R={shape32[0]}>, {shape32[1]} items/SM" if shape32 else ""))
+    metric = METRIC if args.workload == "headline" else \
+        f"pair-evals/s loglik+grad, {args.workload}: FP32-comp vs FP64 plain"
     out = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "metric": metric, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step32, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 pair terms (compensated), f64 reductions", "data": "synthetic",
-        "config": {"workload": f"uniform N={N} D=2, 20x20 km, [0,8760) h sorted, seed {SEED}, "
-                               "base params; log-likelihood + 6-parameter gradient",
-                   "N": N, "D": 2, "precision": "fp32-compensated",
-                   "l2": "flushed before every timed step (256 MiB write, outside the timing)",
-                   "parallelism": f"replicas x{world}"},
+        "config": dict({"workload": w["desc"], "precision": "fp32-compensated",
+                        "l2": "flushed before every timed step (256 MiB write, outside the "
+                              "timing)",
+                        "parallelism": f"replicas x{world}"}, **w["config"]),
         "fp64_plain": {"value": value64, "ms_per_step": ms_step64,
-                       "sweep_ms": statistics.mean(sweep64),
+                       "sweep_ms": statistics.mean(sweep64), "steps": steps64,
                        "terms": {"background": nb64, "self_excitation": ns64}},
         "speedup_fp32c_vs_fp64": value / value64,
         "accuracy": acc,
@@ -385,8 +473,7 @@ def ours_arm(args):
                   "note": "pair terms the sweep evaluated; the rest are the non-causal half of "
                           "the self-excitation sum and tile pairs whose terms are all exactly "
                           "zero in FP32"},
-        "roofline": {"bound": "fp32",
-                     "kernel": f"sweep_f32c_kernel<D=2, R={shape32[0]}>, {shape32[1]} items/SM",
+        "roofline": {"bound": "fp32", "kernel": kernel,
                      "achieved": achieved, "peak": peak_inst, "unit": "Tinst/s",
                      "frac": achieved / peak_inst, "traffic": traffic,
                      "count": "FP32-pipe instructions, FMA = 1: 11 per background term + 5 per "
@@ -396,7 +483,7 @@ def ours_arm(args):
                                     f"(sm_max_mhz, {peak_src})",
                      "sweep_ms": sweep_mean},
         "e2e": {"value": world * pairs / e2e_s, "unit": UNIT,
-                "h2d_bytes_per_step": N * 2 * 8 + N * 8 + N * 4, "d2h_bytes_per_step": 64},
+                "h2d_bytes_per_step": w["h2d"], "d2h_bytes_per_step": w["d2h"]},
         "gpu_launches": launches * args.steps,
         "clocks": clock_summary,
     }
@@ -413,6 +500,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--n", type=int, default=N_EVENTS, help=argparse.SUPPRESS)
+    ap.add_argument("--workload", default="headline",
+                    choices=("headline", "batched", "uneven", "clustered"),
+                    help="headline (default): the metric's N=100k workload; the others are "
+                         "the batched-proposal, uneven-set and clustered configurations")
+    ap.add_argument("--steps64", type=int, default=0,
+                    help="timed steps of the FP64 comparison (default: --steps)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":

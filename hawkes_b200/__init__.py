@@ -6,12 +6,12 @@ the C ABI in include/hphc.h); this package is its Python host interface.
 from .engine import (  # noqa: F401
     AVX, AVX512, COMPENSATED, CUDA, FLOAT, FP32_FAST_EXP, FP32_SPACE_HILO, NO_UNDERFLOW_SKIP,
     OPENCL, PARAMETER_NAMES,
-    PRECISION_FP32_COMP, PRECISION_FP64, SSE, TBB, CudaHawkes, Engine, HawkesError,
+    PRECISION_FP32_COMP, PRECISION_FP64, SSE, TBB, CudaHawkes, Engine, HawkesError, Multiset,
     createEngine, engineInitial, factory, getGradient, getLogLikelihood, getProbsSelfExcite,
     setParameters, setTimesData, updateLocations)
 
 __all__ = [
-    "CudaHawkes", "Engine", "HawkesError", "factory", "createEngine", "engineInitial",
+    "CudaHawkes", "Engine", "HawkesError", "Multiset", "factory", "createEngine", "engineInitial",
     "updateLocations", "setTimesData", "setParameters", "getLogLikelihood",
     "getProbsSelfExcite", "getGradient", "PARAMETER_NAMES",
 ]

@@ -49,7 +49,22 @@ SIGNATURES = {
     "hphc_set_sweep_shape": (ctypes.c_int, [_handle, ctypes.c_int, ctypes.c_int]),
     "hphc_get_sweep_shape": (ctypes.c_int, [_handle, _c_int_p, _c_int_p]),
     "hphc_get_kernel_times": (ctypes.c_int, [_handle, ctypes.POINTER(ctypes.c_float),
+                                             ctypes.POINTER(ctypes.c_float),
                                              ctypes.POINTER(ctypes.c_float)]),
+    "hphc_multiset_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _c_int_p, ctypes.c_long,
+                                            ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    "hphc_multiset_destroy": (None, [_handle]),
+    "hphc_multiset_last_error": (ctypes.c_char_p, [_handle]),
+    "hphc_multiset_set_data": (ctypes.c_int, [_handle, ctypes.c_int, _c_double_p, ctypes.c_size_t,
+                                              _c_double_p, ctypes.c_size_t]),
+    "hphc_multiset_log_likelihood_and_gradient": (ctypes.c_int, [_handle, _c_double_p, _c_double_p,
+                                                                 _c_double_p]),
+    "hphc_multiset_set_kernel_timing": (ctypes.c_int, [_handle, ctypes.c_int]),
+    "hphc_multiset_get_kernel_times": (ctypes.c_int, [_handle, ctypes.POINTER(ctypes.c_float),
+                                                      ctypes.POINTER(ctypes.c_float),
+                                                      ctypes.POINTER(ctypes.c_float)]),
+    "hphc_multiset_get_last_launch_stats": (ctypes.c_int, [_handle, _c_int_p, _c_double_p,
+                                                           _c_double_p]),
 }
 
 

@@ -1,0 +1,618 @@
+// Work-list executor (see hphc_executor.h).
+#include "hphc_executor.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
+
+#include "hphc.h"
+
+namespace hphc {
+namespace {
+
+constexpr double kInvSqrt2Pi = 0.398942280401432677939946059934;
+constexpr double kLog2e = 1.44269504088896340735992468100189214;
+constexpr double kTwoPi = 6.28318530717958647692528676655900577;
+
+// Underflow thresholds (natural-log units) for the tile-pair skip.  FP32:
+// both exponentials return +0 for any argument below -126.5 (log2 units); a
+// true exponent <= -88 is <= -126.96 in log2 units, which the FP32 rounding
+// of the computed exponent (relative ~1e-6) cannot lift above -126.5.  FP64:
+// exp(x) is +0 for x < -745.14; -760 leaves a wide margin.
+constexpr double kSkipF32 = 88.0;
+constexpr double kSkipF64 = 760.0;
+
+size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
+
+void split_float(double x, float& hi, float& lo) {
+    hi = (float)x;
+    lo = (float)(x - (double)hi);
+}
+
+double record_scale(double precisionParam) {
+    return std::fabs(precisionParam) * std::sqrt(0.5 * kLog2e);
+}
+
+// Host replica of the kernel's tile-pair decision (hphc_kernels.cu, tile_mode).
+void tile_needs(double tminI, double tmaxI, double tminJ, double tmaxJ, const PairConsts& c,
+                bool* doB, bool* doS) {
+    const double dtLo = tminI - tmaxJ, dtHi = tmaxI - tminJ;
+    const double minAbs = dtLo > 0.0 ? dtLo : (dtHi < 0.0 ? -dtHi : 0.0);
+    *doB = !(c.skipB >= 0.0 && -c.cB * minAbs * minAbs >= c.skipB);
+    const bool allCausal = dtLo > 0.0;
+    *doS = (dtHi > 0.0) && !(c.skipS >= 0.0 && allCausal && -c.cW * dtLo >= c.skipS);
+}
+
+int f32_stride(int D) {
+    return (2 * (D + 1) + 1 + 3) / 4 * 4;
+}
+
+// Autotuned sweep shapes per process: (D, precision, variant, log2 of the
+// pair count, log2 of the problem count) -> (R, items per SM).
+std::mutex gTuneMutex;
+std::map<std::tuple<int, int, int, int, int>, std::pair<int, int>> gTuneCache;
+
+int log2_bucket(double x) {
+    int b = 0;
+    while (x > 1.0 && b < 80) {
+        x *= 0.5;
+        ++b;
+    }
+    return b;
+}
+
+}  // namespace
+
+int Executor::cuda_fail(cudaError_t e, const char* what) {
+    error = std::string(what) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? HPHC_ERR_OUT_OF_MEMORY : HPHC_ERR_CUDA;
+}
+
+int Executor::init(int D, int precision, int variant, bool underflowSkip, int device,
+                   cudaStream_t stream, float ex2Fix) {
+    D_ = D;
+    precision_ = precision;
+    variant_ = variant;
+    skip_ = underflowSkip;
+    device_ = device;
+    stream_ = stream;
+    ex2Fix_ = ex2Fix;
+    cudaDeviceGetAttribute(&numSMs_, cudaDevAttrMultiProcessorCount, device);
+    R = precision == HPHC_PRECISION_FP64 ? 2 : 4;
+    itemsPerSM = 32;
+    cudaError_t e = cudaMalloc(&dCounter_, sizeof(int));
+    if (e != cudaSuccess) return cuda_fail(e, "device allocation");
+    for (auto& ev : ev_)
+        if ((e = cudaEventCreate(&ev)) != cudaSuccess) return cuda_fail(e, "create events");
+    return HPHC_OK;
+}
+
+void Executor::drop_graph() {
+    if (graphExec_) cudaGraphExecDestroy(graphExec_);
+    graphExec_ = nullptr;
+    graphKey_ = GraphKey{};
+}
+
+void Executor::release() {
+    drop_graph();
+    if (dTables_) cudaFree(dTables_);
+    if (hStaging_) cudaFreeHost(hStaging_);
+    if (dRecPool_) cudaFree(dRecPool_);
+    if (dPartials_) cudaFree(dPartials_);
+    if (dBlockSums_) cudaFree(dBlockSums_);
+    if (dOut_) cudaFree(dOut_);
+    if (hOut_) cudaFreeHost(hOut_);
+    if (dCounter_) cudaFree(dCounter_);
+    for (auto& ev : ev_)
+        if (ev) cudaEventDestroy(ev);
+    dTables_ = hStaging_ = nullptr;
+    dRecPool_ = nullptr;
+    dPartials_ = dBlockSums_ = dOut_ = hOut_ = nullptr;
+    dCounter_ = nullptr;
+    tablesCap_ = stagingCap_ = recCap_ = partialsCap_ = blockCap_ = outCap_ = 0;
+    for (auto& ev : ev_) ev = nullptr;
+}
+
+PairConsts Executor::pair_consts(const double* p) const {
+    const double sigma = p[0], a = p[1], b = p[2], omega = p[3];
+    PairConsts c{};
+    c.cA = -0.5 * a * a;
+    c.cB = -0.5 * b * b;
+    c.cS = -0.5 * sigma * sigma;
+    c.cW = -omega;
+    if (precision_ != HPHC_PRECISION_FP64) {
+        const double sT = record_scale(b);
+        split_float(-(sigma * sigma) / (a * a), c.fSh, c.fSl);
+        split_float(-omega * kLog2e / sT, c.fWh, c.fWl);
+    }
+    c.ex2Fix = (precision_ == HPHC_PRECISION_FP64 || (variant_ & 2)) ? 0.0f : ex2Fix_;
+    const double thr = precision_ == HPHC_PRECISION_FP64 ? kSkipF64 : kSkipF32;
+    c.skipB = (skip_ && c.cB < 0.0 && c.cA <= 0.0) ? thr : -1.0;
+    c.skipS = (skip_ && c.cW < 0.0 && c.cS <= 0.0) ? thr : -1.0;
+    return c;
+}
+
+FinishConsts Executor::finish_consts(const double* p, const SetView& set) const {
+    FinishConsts f{};
+    f.sigma = p[0];
+    f.a = p[1];
+    f.b = p[2];
+    f.omega = p[3];
+    f.theta = p[4];
+    f.mu0 = p[5];
+    f.bgScale = std::pow(f.a, D_) * f.b / kTwoPi;
+    f.seScale = f.omega * std::pow(f.sigma, D_) * kInvSqrt2Pi;
+    f.prefB = f.mu0 * f.bgScale;
+    f.prefS = f.theta * f.seScale;
+    for (int q = 0; q < kNumAcc; ++q) f.accScale[q] = 1.0;
+    if (precision_ != HPHC_PRECISION_FP64) {
+        const double sX = record_scale(f.a), sT = record_scale(f.b);
+        f.accScale[1] = f.accScale[4] = 1.0 / (sX * sX);  // sums of d'^2
+        f.accScale[2] = 1.0 / (sT * sT);                  // sum of dt'^2
+        f.accScale[5] = 1.0 / sT;                         // sum of dt'
+    }
+    f.T = set.hTimes[set.N - 1];
+    // src/NewHawkes.hpp:659: locationCount * (embeddingDimension - 1) * log(M_1_SQRT_2PI)
+    f.constant = (double)(set.N * (D_ - 1)) * std::log(kInvSqrt2Pi);
+    f.D = D_;
+    return f;
+}
+
+int Executor::sweep_grid(int r) const {
+    const int perSM = sweep_list_blocks_per_sm(precision_ == HPHC_PRECISION_FP64 ? 0 : 1, D_, r,
+                                               variant_);
+    return numSMs_ * std::max(1, perSM);
+}
+
+int Executor::build_plan(const std::vector<SetView>& sets, const int* setOf, const double* params,
+                         int P, double* dProbs, int r, int items) {
+    Plan& pl = plan_;
+    pl.P = P;
+    pl.setOf.assign(setOf, setOf + P);
+    pl.sp.assign(P, SweepProblem{});
+    pl.fp.assign(P, FinishProblem{});
+    pl.pj.clear();
+    pl.items.clear();
+    pl.stripChunks.clear();
+    pl.fb.clear();
+    pl.maxN = 0;
+    const bool fp32 = precision_ != HPHC_PRECISION_FP64;
+    const int stripEvents = kSweepThreads * r;
+    const int S32 = f32_stride(D_);
+
+    double totalStrips = 0.0;
+    for (int p = 0; p < P; ++p) {
+        const SetView& s = sets[setOf[p]];
+        totalStrips += (s.N + stripEvents - 1) / stripEvents;
+    }
+    const int target = numSMs_ * items;
+    const int nChunksTarget = std::max(1, (int)std::ceil(target / std::max(1.0, totalStrips)));
+
+    size_t recOff = 0, partOff = 0;
+    std::vector<size_t> chunkBase(P);
+    int blockBase = 0;
+    for (int p = 0; p < P; ++p) {
+        const SetView& s = sets[setOf[p]];
+        const double* prm = params + (size_t)6 * p;
+        if (fp32 && !(prm[1] != 0.0 && prm[2] != 0.0 && std::isfinite(prm[1]) &&
+                      std::isfinite(prm[2]))) {
+            char buf[200];
+            snprintf(buf, sizeof buf,
+                     "FP32-compensated mode needs finite non-zero tauXprec and tauTprec (problem "
+                     "%d: %g, %g); use the FP64 mode", p, prm[1], prm[2]);
+            error = buf;
+            return HPHC_ERR_UNSUPPORTED;
+        }
+        const int N = s.N;
+        const int nTiles = (N + kTile - 1) / kTile;
+        const int nStrips = (N + stripEvents - 1) / stripEvents;
+        const int Npad = nStrips * stripEvents;
+        const int CT = std::max(1, (nTiles + nChunksTarget - 1) / nChunksTarget);  // tiles a chunk
+        const int maxChunks = (nTiles + CT - 1) / CT;
+        pl.maxN = std::max(pl.maxN, N);
+        SweepProblem& sp = pl.sp[p];
+        sp.c = pair_consts(prm);
+        sp.N = N;
+        sp.nTiles = nTiles;
+        sp.Npad = Npad;
+        sp.tileMin = s.dTileMin;
+        sp.tileMax = s.dTileMax;
+        sp.partials = reinterpret_cast<double*>(partOff);  // offset, fixed up later
+        partOff += (size_t)maxChunks * kNumAcc * Npad;
+        if (fp32) {
+            sp.rec = reinterpret_cast<const void*>(recOff);  // offset, fixed up later
+            PackJob j{};
+            j.loc = s.dLoc;
+            j.times = s.dTimes;
+            j.ranks = s.dRanks;
+            j.rec = reinterpret_cast<float*>(recOff);
+            j.sX = record_scale(prm[1]);
+            j.sT = record_scale(prm[2]);
+            j.N = N;
+            pl.pj.push_back(j);
+            recOff += (size_t)N * S32;
+        } else {
+            sp.rec = s.dRecF64;
+        }
+
+        // work items: each strip's band of tiles that may hold a non-zero term
+        chunkBase[p] = pl.stripChunks.size();
+        for (int st = 0; st < nStrips; ++st) {
+            const int ts0 = st * r, ts1 = std::min(ts0 + r, nTiles);
+            double tminI = INFINITY, tmaxI = -INFINITY;
+            for (int t = ts0; t < ts1; ++t) {
+                tminI = std::min(tminI, s.hTileMin[t]);
+                tmaxI = std::max(tmaxI, s.hTileMax[t]);
+            }
+            int lo = 0, hi = nTiles;
+            if (s.sorted) {
+                auto needed = [&](int jt) {
+                    bool b, se;
+                    tile_needs(tminI, tmaxI, s.hTileMin[jt], s.hTileMax[jt], sp.c, &b, &se);
+                    return b || se;
+                };
+                // left of the strip the test is non-decreasing in jt, right of
+                // it non-increasing (times ascending); keep one tile of margin
+                int a = 0, b = ts0;
+                while (a < b) {
+                    const int m = (a + b) / 2;
+                    if (needed(m)) b = m; else a = m + 1;
+                }
+                lo = std::max(0, a - 1);
+                a = ts1;
+                b = nTiles;
+                while (a < b) {
+                    const int m = (a + b) / 2;
+                    if (needed(m)) a = m + 1; else b = m;
+                }
+                hi = std::min(nTiles, a + 1);
+            }
+            // Chunks sit on a fixed grid of CT tiles per problem, so a tile
+            // always lands in the same chunk whatever the band: skipping a
+            // band's outside only drops chunks whose sums are exactly zero,
+            // and the FP64 chunk sums are added in the same order either way.
+            const int cFirst = lo / CT, cLast = (hi - 1) / CT + 1;
+            for (int c = cFirst; c < cLast; ++c) {
+                WorkItem w{};
+                w.problem = p;
+                w.strip = st;
+                w.jt0 = std::max(lo, c * CT);
+                w.jt1 = std::min(hi, (c + 1) * CT);
+                w.slot = c - cFirst;
+                pl.items.push_back(w);
+            }
+            pl.stripChunks.push_back(cLast - cFirst);
+        }
+
+        FinishProblem& fp = pl.fp[p];
+        fp.partials = nullptr;  // fixed up later
+        fp.stripChunks = nullptr;
+        fp.times = s.dTimes;
+        fp.probs = (p == 0) ? dProbs : nullptr;
+        fp.N = N;
+        fp.Npad = Npad;
+        fp.stripEvents = stripEvents;
+        fp.blockBase = blockBase;
+        fp.nBlocks = finish_blocks(N);
+        fp.f = finish_consts(prm, s);
+        for (int b = 0; b < fp.nBlocks; ++b) pl.fb.push_back(FinishBlock{p, b * kFinishThreads});
+        blockBase += fp.nBlocks;
+    }
+    pl.nBlocks = blockBase;
+    std::stable_sort(pl.items.begin(), pl.items.end(), [](const WorkItem& x, const WorkItem& y) {
+        return (x.jt1 - x.jt0) > (y.jt1 - y.jt0);
+    });
+
+    // table layout and buffer capacities
+    offSP_ = 0;
+    offItems_ = align16(offSP_ + sizeof(SweepProblem) * P);
+    const size_t nItems = pl.items.size();
+    itemsCap_ = std::max(itemsCap_, nItems);
+    offNItems_ = align16(offItems_ + sizeof(WorkItem) * itemsCap_);
+    offChunks_ = align16(offNItems_ + sizeof(int));
+    offFP_ = align16(offChunks_ + sizeof(int) * pl.stripChunks.size());
+    offFB_ = align16(offFP_ + sizeof(FinishProblem) * P);
+    offPJ_ = align16(offFB_ + sizeof(FinishBlock) * pl.fb.size());
+    tablesBytes_ = align16(offPJ_ + sizeof(PackJob) * pl.pj.size());
+
+    recNeed_ = recOff;
+    partialsNeed_ = partOff;
+    int st = ensure_buffers();
+    if (st) return st;
+
+    // fix up offsets into device pointers and fill the staging buffer
+    char* h = static_cast<char*>(hStaging_);
+    char* d = static_cast<char*>(dTables_);
+    for (int p = 0; p < P; ++p) {
+        SweepProblem& sp = pl.sp[p];
+        const size_t po = reinterpret_cast<size_t>(sp.partials);
+        sp.partials = dPartials_ + po;
+        if (fp32) sp.rec = dRecPool_ + reinterpret_cast<size_t>(sp.rec);
+        FinishProblem& fp = pl.fp[p];
+        fp.partials = sp.partials;
+        fp.stripChunks = reinterpret_cast<const int*>(d + offChunks_) + chunkBase[p];
+    }
+    for (auto& j : pl.pj) j.rec = dRecPool_ + reinterpret_cast<size_t>(j.rec);
+    std::memcpy(h + offSP_, pl.sp.data(), sizeof(SweepProblem) * P);
+    std::memcpy(h + offItems_, pl.items.data(), sizeof(WorkItem) * nItems);
+    const int n = (int)nItems;
+    std::memcpy(h + offNItems_, &n, sizeof(int));
+    std::memcpy(h + offChunks_, pl.stripChunks.data(), sizeof(int) * pl.stripChunks.size());
+    std::memcpy(h + offFP_, pl.fp.data(), sizeof(FinishProblem) * P);
+    std::memcpy(h + offFB_, pl.fb.data(), sizeof(FinishBlock) * pl.fb.size());
+    if (!pl.pj.empty()) std::memcpy(h + offPJ_, pl.pj.data(), sizeof(PackJob) * pl.pj.size());
+    return HPHC_OK;
+}
+
+int Executor::ensure_buffers() {
+    const Plan& pl = plan_;
+    bool grew = false;
+    cudaError_t e = cudaSuccess;
+    auto grow_dev = [&](void** ptr, size_t& cap, size_t needBytes) -> cudaError_t {
+        if (needBytes <= cap && *ptr) return cudaSuccess;
+        const size_t n = std::max<size_t>(needBytes + needBytes / 4, 256);
+        if (*ptr) cudaFree(*ptr);
+        *ptr = nullptr;
+        cap = 0;
+        const cudaError_t err = cudaMalloc(ptr, n);
+        if (err == cudaSuccess) cap = n;
+        grew = true;
+        return err;
+    };
+    if ((e = grow_dev(reinterpret_cast<void**>(&dRecPool_), recCap_,
+                      std::max<size_t>(recNeed_, 1) * sizeof(float))) != cudaSuccess ||
+        (e = grow_dev(reinterpret_cast<void**>(&dPartials_), partialsCap_,
+                      std::max<size_t>(partialsNeed_, 1) * sizeof(double))) != cudaSuccess ||
+        (e = grow_dev(reinterpret_cast<void**>(&dBlockSums_), blockCap_,
+                      (size_t)std::max(pl.nBlocks, 1) * 8 * sizeof(double))) != cudaSuccess ||
+        (e = grow_dev(&dTables_, tablesCap_, tablesBytes_)) != cudaSuccess)
+        return cuda_fail(e, "device allocation");
+    if (stagingCap_ < tablesCap_) {
+        if (hStaging_) cudaFreeHost(hStaging_);
+        hStaging_ = nullptr;
+        stagingCap_ = 0;
+        if ((e = cudaMallocHost(&hStaging_, tablesCap_)) != cudaSuccess)
+            return cuda_fail(e, "pinned allocation");
+        stagingCap_ = tablesCap_;
+        grew = true;
+    }
+    if (outCap_ < (size_t)pl.P * 8) {
+        if (dOut_) cudaFree(dOut_);
+        if (hOut_) cudaFreeHost(hOut_);
+        dOut_ = hOut_ = nullptr;
+        outCap_ = 0;
+        const size_t n = (size_t)pl.P * 8;
+        if ((e = cudaMalloc(&dOut_, n * sizeof(double))) != cudaSuccess ||
+            (e = cudaMallocHost(&hOut_, n * sizeof(double))) != cudaSuccess)
+            return cuda_fail(e, "device allocation");
+        outCap_ = n;
+        grew = true;
+    }
+    if (grew) drop_graph();
+    return HPHC_OK;
+}
+
+// Timing events: inside a stream capture an event is only recorded as a graph
+// node (and so usable for elapsed times) when marked external.
+cudaError_t Executor::record(cudaEvent_t ev) {
+    return capturing_ ? cudaEventRecordWithFlags(ev, stream_, cudaEventRecordExternal)
+                      : cudaEventRecord(ev, stream_);
+}
+
+// The stage sequence of one run on stream_ (also what the graph captures).
+int Executor::launch_sequence(int grid) {
+    const Plan& pl = plan_;
+    const int prec = precision_ == HPHC_PRECISION_FP64 ? 0 : 1;
+    char* d = static_cast<char*>(dTables_);
+    const auto* sp = reinterpret_cast<const SweepProblem*>(d + offSP_);
+    const auto* items = reinterpret_cast<const WorkItem*>(d + offItems_);
+    const auto* nItems = reinterpret_cast<const int*>(d + offNItems_);
+    const auto* fp = reinterpret_cast<const FinishProblem*>(d + offFP_);
+    const auto* fb = reinterpret_cast<const FinishBlock*>(d + offFB_);
+    const auto* pj = reinterpret_cast<const PackJob*>(d + offPJ_);
+    cudaError_t e = cudaSuccess;
+    int launches = 0;
+    if (kernelTiming && (e = record(ev_[0]))) return cuda_fail(e, "timing event");
+    if ((e = cudaMemcpyAsync(dTables_, hStaging_, tablesBytes_, cudaMemcpyHostToDevice, stream_)))
+        return cuda_fail(e, "stage tables");
+    if (prec == 1) {
+        if ((e = launch_pack_f32_jobs(D_, pl.P, pl.maxN, pj, stream_)))
+            return cuda_fail(e, "pack kernel");
+        ++launches;
+    }
+    if ((e = cudaMemsetAsync(dCounter_, 0, sizeof(int), stream_)))
+        return cuda_fail(e, "reset work counter");
+    if (kernelTiming && (e = record(ev_[1]))) return cuda_fail(e, "timing event");
+    if ((e = launch_sweep_list(prec, D_, R, variant_, grid, sp, items, nItems, dCounter_, stream_)))
+        return cuda_fail(e, "sweep kernel");
+    if (kernelTiming && (e = record(ev_[2]))) return cuda_fail(e, "timing event");
+    if ((e = launch_finish_list(pl.nBlocks, fp, fb, dBlockSums_, stream_)))
+        return cuda_fail(e, "finish kernel");
+    if ((e = launch_final_list(pl.P, fp, dBlockSums_, dOut_, stream_)))
+        return cuda_fail(e, "final kernel");
+    launches += 3;
+    if ((e = cudaMemcpyAsync(hOut_, dOut_, (size_t)pl.P * 8 * sizeof(double),
+                             cudaMemcpyDeviceToHost, stream_)))
+        return cuda_fail(e, "read results");
+    if (kernelTiming && (e = record(ev_[3]))) return cuda_fail(e, "timing event");
+    lastLaunches = launches;
+    return HPHC_OK;
+}
+
+int Executor::autotune(const std::vector<SetView>& sets, const int* setOf, const double* params,
+                       int P, double* dProbs) {
+    double pairs = 0.0;
+    for (int p = 0; p < P; ++p) pairs += (double)sets[setOf[p]].N * sets[setOf[p]].N;
+    const auto key = std::make_tuple(D_, precision_, variant_, log2_bucket(pairs), log2_bucket(P));
+    {
+        std::lock_guard<std::mutex> lock(gTuneMutex);
+        auto it = gTuneCache.find(key);
+        if (it != gTuneCache.end()) {
+            R = fixedR ? fixedR : it->second.first;
+            itemsPerSM = fixedItems ? fixedItems : it->second.second;
+            tuned_ = true;
+            return HPHC_OK;
+        }
+    }
+    std::vector<int> rs, its;
+    if (fixedR) rs = {fixedR};
+    else if (precision_ == HPHC_PRECISION_FP64) rs = {1, 2};
+    else rs = {2, 4};
+    if (fixedItems) its = {fixedItems};
+    else its = {8, 16, 32, 64};
+    const bool timing = kernelTiming;
+    kernelTiming = true;
+    float best = 1e30f;
+    int bestR = rs[0], bestI = its[0];
+    int st = HPHC_OK;
+    for (int r : rs) {
+        for (int it : its) {
+            R = r;
+            itemsPerSM = it;
+            if ((st = build_plan(sets, setOf, params, P, dProbs, r, it))) break;
+            const int grid = sweep_grid(r);
+            for (int rep = 0; rep < 2 && !st; ++rep) st = launch_sequence(grid);
+            if (st) break;
+            cudaError_t e = cudaStreamSynchronize(stream_);
+            if (e != cudaSuccess) {
+                st = cuda_fail(e, "autotune");
+                break;
+            }
+            float ms = 0.f;
+            if ((e = cudaEventElapsedTime(&ms, ev_[1], ev_[2])) != cudaSuccess) {
+                st = cuda_fail(e, "autotune timing");
+                break;
+            }
+            if (ms < best) {
+                best = ms;
+                bestR = r;
+                bestI = it;
+            }
+        }
+        if (st) break;
+    }
+    kernelTiming = timing;
+    if (st) return st;
+    {
+        std::lock_guard<std::mutex> lock(gTuneMutex);
+        gTuneCache[key] = {bestR, bestI};
+    }
+    R = bestR;
+    itemsPerSM = bestI;
+    tuned_ = true;
+    return HPHC_OK;
+}
+
+int Executor::enqueue(const std::vector<SetView>& sets, const int* setOf, const double* params,
+                      int P, double* dProbs) {
+    if (P < 1) {
+        error = "no problems to evaluate";
+        return HPHC_ERR_BAD_ARGUMENT;
+    }
+    if (fixedR && fixedItems) {
+        R = fixedR;
+        itemsPerSM = fixedItems;
+        tuned_ = true;
+    }
+    if (!tuned_) {
+        const int st = autotune(sets, setOf, params, P, dProbs);
+        if (st) return st;
+    }
+    int st = build_plan(sets, setOf, params, P, dProbs, R, itemsPerSM);
+    if (st) return st;
+    const int grid = sweep_grid(R);
+    timedValid = false;
+    if (!useGraph) {
+        st = launch_sequence(grid);
+        timedValid = kernelTiming && st == HPHC_OK;
+        return st;
+    }
+    GraphKey key;
+    key.P = plan_.P;
+    key.nBlocks = plan_.nBlocks;
+    key.maxN = plan_.maxN;
+    key.R = R;
+    key.grid = grid;
+    key.tablesBytes = tablesBytes_;
+    key.tables = dTables_;
+    key.timing = kernelTiming;
+    const bool same = graphExec_ && key.P == graphKey_.P && key.nBlocks == graphKey_.nBlocks &&
+                      key.maxN == graphKey_.maxN && key.R == graphKey_.R &&
+                      key.grid == graphKey_.grid && key.tablesBytes == graphKey_.tablesBytes &&
+                      key.tables == graphKey_.tables && key.timing == graphKey_.timing;
+    cudaError_t e;
+    if (!same) {
+        drop_graph();
+        cudaGraph_t graph = nullptr;
+        if ((e = cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal)))
+            return cuda_fail(e, "begin graph capture");
+        capturing_ = true;
+        st = launch_sequence(grid);
+        capturing_ = false;
+        e = cudaStreamEndCapture(stream_, &graph);
+        if (st) {
+            if (graph) cudaGraphDestroy(graph);
+            return st;
+        }
+        if (e != cudaSuccess) return cuda_fail(e, "end graph capture");
+        e = cudaGraphInstantiate(&graphExec_, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+            graphExec_ = nullptr;
+            return cuda_fail(e, "instantiate graph");
+        }
+        graphKey_ = key;
+    }
+    if ((e = cudaGraphLaunch(graphExec_, stream_))) return cuda_fail(e, "launch graph");
+    lastLaunches = (precision_ == HPHC_PRECISION_FP64 ? 3 : 4);
+    timedValid = kernelTiming;
+    return HPHC_OK;
+}
+
+int Executor::wait(double* hostOut) {
+    const cudaError_t e = cudaStreamSynchronize(stream_);
+    if (e != cudaSuccess) return cuda_fail(e, "evaluation");
+    if (hostOut) std::memcpy(hostOut, hOut_, (size_t)plan_.P * 8 * sizeof(double));
+    if (timedValid) {
+        cudaError_t t;
+        if ((t = cudaEventElapsedTime(&lastSweepMs, ev_[1], ev_[2])) != cudaSuccess ||
+            (t = cudaEventElapsedTime(&lastFinishMs, ev_[2], ev_[3])) != cudaSuccess ||
+            (t = cudaEventElapsedTime(&lastStepMs, ev_[0], ev_[3])) != cudaSuccess) {
+            timedValid = false;
+            return cuda_fail(t, "kernel timing");
+        }
+    }
+    return HPHC_OK;
+}
+
+void Executor::count_terms(const std::vector<SetView>& sets, double* bTerms,
+                           double* sTerms) const {
+    double nb = 0.0, ns = 0.0;
+    const int stripEvents = kSweepThreads * R;
+    for (const WorkItem& w : plan_.items) {
+        const SetView& s = sets[plan_.setOf[w.problem]];
+        const PairConsts& c = plan_.sp[w.problem].c;
+        const int nTiles = plan_.sp[w.problem].nTiles;
+        const int ts0 = w.strip * R, ts1 = std::min(ts0 + R, nTiles);
+        double tminI = INFINITY, tmaxI = -INFINITY;
+        for (int t = ts0; t < ts1; ++t) {
+            tminI = std::min(tminI, s.hTileMin[t]);
+            tmaxI = std::max(tmaxI, s.hTileMax[t]);
+        }
+        const double ni = std::min(stripEvents, s.N - w.strip * stripEvents);
+        for (int jt = w.jt0; jt < w.jt1; ++jt) {
+            bool b, se;
+            tile_needs(tminI, tmaxI, s.hTileMin[jt], s.hTileMax[jt], c, &b, &se);
+            const double nj = std::min(kTile, s.N - jt * kTile);
+            if (b) nb += ni * nj;
+            if (se) ns += ni * nj;
+        }
+    }
+    *bTerms = nb;
+    *sTerms = ns;
+}
+
+}  // namespace hphc

@@ -1,0 +1,145 @@
+// Work-list executor: evaluates any number of problems (an event set at a
+// parameter vector) with one launch per stage.
+//
+//   stage   what                                          launch
+//   H2D     problem tables, work items, finish tables    one cudaMemcpyAsync from pinned staging
+//   pack    FP32 records scaled per problem (FP32 mode)   pack_f32_jobs_kernel, grid (N, P)
+//   sweep   persistent CTAs over the work list            sweep_*_list_kernel
+//   finish  per-event contributions, per-CTA sums        finish_list_kernel
+//   final   per-problem fixed-order totals               final_list_kernel
+//   D2H     P x 8 results                                 one cudaMemcpyAsync to pinned memory
+//
+// The sequence is captured once into a CUDA graph and replayed while buffer
+// capacities and the sweep shape stay the same; only the staged tables change
+// between runs.  Work items cover each strip's band of tiles that can hold a
+// non-zero term (found on the host from per-tile time bounds with the same
+// test the kernel applies), split into equal chunks and listed largest first.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "hphc_kernels.cuh"
+
+namespace hphc {
+
+// An event set resident on the device, with host copies used for planning.
+struct SetView {
+    int N = 0;
+    const double* dLoc = nullptr;      // N x D raw coordinates
+    const double* dTimes = nullptr;    // N raw times
+    const int32_t* dRanks = nullptr;   // dense time ranks (FP32 mode)
+    const double* dRecF64 = nullptr;   // FP64 records (FP64 mode)
+    const double* dTileMin = nullptr;  // per-tile time bounds
+    const double* dTileMax = nullptr;
+    const double* hTimes = nullptr;    // host copies
+    const double* hTileMin = nullptr;
+    const double* hTileMax = nullptr;
+    bool sorted = false;               // times ascending (bands are contiguous)
+};
+
+struct RunStats {
+    int launches = 0;        // kernels launched by the last run
+    double bTerms = 0.0;     // background pair terms the sweep evaluated
+    double sTerms = 0.0;     // self-excitation pair terms the sweep evaluated
+};
+
+class Executor {
+public:
+    // precision: HPHC_PRECISION_*; variant: FP32 variant bits (see
+    // hphc_kernels.cu); ex2Fix: exponent offset for the hardware exponential.
+    int init(int D, int precision, int variant, bool underflowSkip, int device, cudaStream_t stream,
+             float ex2Fix);
+    void release();
+
+    // Plan and enqueue P problems (problem p = set setOf[p] at params[6p..6p+5])
+    // without waiting.  dProbs: device buffer receiving P_i of problem 0, or null.
+    int enqueue(const std::vector<SetView>& sets, const int* setOf, const double* params, int P,
+                double* dProbs);
+    // Wait for the last enqueue and copy its P x 8 results (log-likelihood,
+    // gradient, 0) to hostOut.
+    int wait(double* hostOut);
+
+    // Pair terms the last run's sweep evaluated (replays the tile decisions).
+    void count_terms(const std::vector<SetView>& sets, double* bTerms, double* sTerms) const;
+
+    std::string error;
+    int fixedR = 0, fixedItems = 0;  // sweep shape overrides; 0 = autotune
+    int R = 2, itemsPerSM = 16;      // shape in use
+    bool useGraph = true;
+    bool kernelTiming = false;
+    float lastSweepMs = 0.f, lastFinishMs = 0.f, lastStepMs = 0.f;
+    bool timedValid = false;
+    int lastLaunches = 0;
+
+private:
+    int D_ = 0, precision_ = 0, variant_ = 0, device_ = 0, numSMs_ = 148;
+    bool skip_ = true;
+    float ex2Fix_ = 0.f;
+    cudaStream_t stream_ = nullptr;
+    bool tuned_ = false;
+
+    // plan of the last enqueue
+    struct Plan {
+        std::vector<SweepProblem> sp;
+        std::vector<WorkItem> items;
+        std::vector<int> stripChunks;   // concatenated over problems
+        std::vector<FinishProblem> fp;
+        std::vector<FinishBlock> fb;
+        std::vector<PackJob> pj;
+        std::vector<int> setOf;
+        int P = 0, maxN = 0, nBlocks = 0;
+    } plan_;
+
+    // device / pinned buffers (capacities grow; a growth invalidates the graph)
+    void* dTables_ = nullptr;
+    size_t tablesCap_ = 0;
+    void* hStaging_ = nullptr;
+    size_t stagingCap_ = 0;
+    float* dRecPool_ = nullptr;
+    size_t recCap_ = 0;
+    double* dPartials_ = nullptr;
+    size_t partialsCap_ = 0;
+    double* dBlockSums_ = nullptr;
+    size_t blockCap_ = 0;
+    double* dOut_ = nullptr;
+    double* hOut_ = nullptr;
+    size_t outCap_ = 0;
+    int* dCounter_ = nullptr;
+    cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
+
+    // table layout inside dTables_ / hStaging_ (byte offsets)
+    size_t offSP_ = 0, offItems_ = 0, offNItems_ = 0, offChunks_ = 0, offFP_ = 0, offFB_ = 0,
+           offPJ_ = 0, tablesBytes_ = 0;
+    size_t itemsCap_ = 0;
+    size_t recNeed_ = 0, partialsNeed_ = 0;  // floats / doubles the last plan needs
+
+    // graph
+    cudaGraphExec_t graphExec_ = nullptr;
+    struct GraphKey {
+        int P = -1, nBlocks = -1, maxN = -1, R = -1, grid = -1;
+        size_t tablesBytes = 0;
+        void* tables = nullptr;
+        bool timing = false;
+    } graphKey_;
+
+    int build_plan(const std::vector<SetView>& sets, const int* setOf, const double* params, int P,
+                   double* dProbs, int r, int items);
+    int ensure_buffers();
+    int launch_sequence(int grid);
+    int sweep_grid(int r) const;
+    int autotune(const std::vector<SetView>& sets, const int* setOf, const double* params, int P,
+                 double* dProbs);
+    int cuda_fail(cudaError_t e, const char* what);
+    void drop_graph();
+    cudaError_t record(cudaEvent_t ev);
+    bool capturing_ = false;
+
+public:
+    PairConsts pair_consts(const double* p) const;
+    FinishConsts finish_consts(const double* p, const SetView& set) const;
+};
+
+}  // namespace hphc

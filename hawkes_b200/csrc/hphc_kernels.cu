@@ -77,6 +77,30 @@ __global__ void pack_f32_kernel(int N, const double* __restrict__ loc,
     for (int k = 2 * D + 3; k < S; ++k) r[k] = 0.0f;
 }
 
+// FP32 records for many problems in one launch: blockIdx.y = job.
+template <int D>
+__global__ void pack_f32_jobs_kernel(const PackJob* __restrict__ jobs) {
+    constexpr int S = Layout<D>::kF32Stride;
+    const PackJob J = jobs[blockIdx.y];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= J.N) return;
+    float* r = J.rec + (size_t)i * S;
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        const double v = J.loc[(size_t)i * D + k] * J.sX;
+        const float h = (float)v;
+        r[k] = h;
+        r[D + 1 + k] = (float)(v - (double)h);
+    }
+    const double v = J.times[i] * J.sT;
+    const float h = (float)v;
+    r[D] = h;
+    r[2 * D + 1] = (float)(v - (double)h);
+    r[2 * D + 2] = __int_as_float(J.ranks[i]);
+#pragma unroll
+    for (int k = 2 * D + 3; k < S; ++k) r[k] = 0.0f;
+}
+
 // One CTA of kTile threads per tile: min and max of t over the tile.
 __global__ void __launch_bounds__(kTile)
 tile_bounds_kernel(int N, const double* __restrict__ times, double* __restrict__ tileMin,
@@ -168,22 +192,23 @@ __device__ __forceinline__ void body_f64(const double* __restrict__ sRec, int nj
     }
 }
 
+// One work item of the FP64 sweep: target strip `strip` (kSweepThreads * R
+// events) against j tiles [jt0, jt1); unit pair sums to partial slot `slot`.
 template <int D, int R>
-__global__ void __launch_bounds__(kSweepThreads)
-sweep_f64_kernel(SweepGeometry g, const double* __restrict__ rec,
-                 const double* __restrict__ tileMin, const double* __restrict__ tileMax,
-                 PairConsts c, double* __restrict__ partials) {
+__device__ __forceinline__ void f64_item(const double* __restrict__ rec,
+                                         const double* __restrict__ tileMin,
+                                         const double* __restrict__ tileMax,
+                                         double* __restrict__ partials, int N, int nTiles,
+                                         int Npad, const PairConsts& c, int strip, int jt0,
+                                         int jt1, int slot, double* sRec) {
     constexpr int S = Layout<D>::kF64Stride;
-    __shared__ __align__(16) double sRec[kTile * S];
     const int tid = threadIdx.x;
-    const int strip = blockIdx.x / g.nChunks;
-    const int chunk = blockIdx.x - strip * g.nChunks;
     const int stripBase = strip * kSweepThreads * R;
 
     double xi[R][D], ti[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-        const int i = min(stripBase + r * kSweepThreads + tid, g.N - 1);
+        const int i = min(stripBase + r * kSweepThreads + tid, N - 1);
 #pragma unroll
         for (int k = 0; k < D; ++k) xi[r][k] = rec[(size_t)i * S + k];
         ti[r] = rec[(size_t)i * S + D];
@@ -192,7 +217,7 @@ sweep_f64_kernel(SweepGeometry g, const double* __restrict__ rec,
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int tt = stripBase / kTile + r;
-        if (tt < g.nTiles) {
+        if (tt < nTiles) {
             tminI = fmin(tminI, tileMin[tt]);
             tmaxI = fmax(tmaxI, tileMax[tt]);
         }
@@ -203,13 +228,11 @@ sweep_f64_kernel(SweepGeometry g, const double* __restrict__ rec,
 #pragma unroll
         for (int q = 0; q < kNumAcc; ++q) acc[r][q] = 0.0;
 
-    const int jt0 = chunk * g.chunkTiles;
-    const int jt1 = min(jt0 + g.chunkTiles, g.nTiles);
     for (int jt = jt0; jt < jt1; ++jt) {
         const TileMode m = tile_mode(tminI, tmaxI, tileMin[jt], tileMax[jt], c);
         if (!m.doB && !m.doS) continue;
         const int j0 = jt * kTile;
-        const int nj = min(kTile, g.N - j0);
+        const int nj = min(kTile, N - j0);
         __syncthreads();
         const double2* src = reinterpret_cast<const double2*>(rec + (size_t)j0 * S);
         double2* dst = reinterpret_cast<double2*>(sRec);
@@ -232,11 +255,54 @@ sweep_f64_kernel(SweepGeometry g, const double* __restrict__ rec,
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int i = stripBase + r * kSweepThreads + tid;
-        if (i < g.N) {
+        if (i < N) {
 #pragma unroll
             for (int q = 0; q < kNumAcc; ++q)
-                partials[((size_t)chunk * kNumAcc + q) * g.Npad + i] = acc[r][q];
+                partials[((size_t)slot * kNumAcc + q) * Npad + i] = acc[r][q];
         }
+    }
+}
+
+// Grid form: one CTA per (strip, chunk), chunks of g.chunkTiles tiles.
+template <int D, int R>
+__global__ void __launch_bounds__(kSweepThreads)
+sweep_f64_kernel(SweepGeometry g, const double* __restrict__ rec,
+                 const double* __restrict__ tileMin, const double* __restrict__ tileMax,
+                 PairConsts c, double* __restrict__ partials) {
+    __shared__ __align__(16) double sRec[kTile * Layout<D>::kF64Stride];
+    const int strip = blockIdx.x / g.nChunks;
+    const int chunk = blockIdx.x - strip * g.nChunks;
+    const int jt0 = chunk * g.chunkTiles;
+    const int jt1 = min(jt0 + g.chunkTiles, g.nTiles);
+    f64_item<D, R>(rec, tileMin, tileMax, partials, g.N, g.nTiles, g.Npad, c, strip, jt0, jt1,
+                   chunk, sRec);
+}
+
+// Takes the next work-list index for the CTA (all threads get the same one).
+__device__ __forceinline__ int next_item(int* counter, int* sNext) {
+    __syncthreads();
+    if (threadIdx.x == 0) *sNext = atomicAdd(counter, 1);
+    __syncthreads();
+    return *sNext;
+}
+
+// Work-list form: persistent CTAs take items until the list is exhausted.
+template <int D, int R>
+__global__ void __launch_bounds__(kSweepThreads)
+sweep_f64_list_kernel(const SweepProblem* __restrict__ problems,
+                      const WorkItem* __restrict__ items, const int* __restrict__ nItems,
+                      int* __restrict__ counter) {
+    __shared__ __align__(16) double sRec[kTile * Layout<D>::kF64Stride];
+    __shared__ int sNext;
+    const int n = *nItems;
+    for (;;) {
+        const int it = next_item(counter, &sNext);
+        if (it >= n) break;
+        const WorkItem w = items[it];
+        const SweepProblem& P = problems[w.problem];
+        const PairConsts c = P.c;
+        f64_item<D, R>(static_cast<const double*>(P.rec), P.tileMin, P.tileMax, P.partials, P.N,
+                       P.nTiles, P.Npad, c, w.strip, w.jt0, w.jt1, w.slot, sRec);
     }
 }
 
@@ -276,17 +342,17 @@ constexpr float kP5 = 0x1.5da248p-10f;
 constexpr float kP6 = 0x1.43ec02p-13f;
 constexpr float kP7 = 0x1.e50106p-17f;
 
-// 2^x for x <= 127 on the FMA pipe: Cody-Waite reduction x = n + f with
-// n = round(x) (added to 1.5 * 2^23 so the integer lands in the low mantissa
-// bits), |f| <= 1/2, p(f) by Horner, and 2^n built directly in the exponent
-// field: bits(t) << 23 == n << 23 (mod 2^32) because the magic constant's bits
-// all shift out.  Arguments below -126.5 give n = -127 and a scale of exactly
-// +0, so the result is +0 as with ex2.approx.ftz and the tile-level underflow
-// skip stays exact.
+// 2^x by Cody-Waite reduction x = n + f, n = rint(x), |f| <= 1/2 (f exact),
+// p(f) by Horner on the FMA pipe, and the scale 2^n from ex2.approx.ftz on the
+// integer n: that instruction returns exactly 2^n for every integer n (checked
+// on the device for n in [-200, 130]), +0 for n <= -127 and +inf above 127, so
+// the scale needs no clamp or exponent-field arithmetic and any |x| is safe
+// (for |x| >= 2^23, f = 0).  Arguments below -126.5 give +0 as with
+// ex2.approx.ftz, so the tile-level underflow skip stays exact.  The hardware
+// approximation error never enters: only the exact power of two is taken from
+// it, the fractional part is the polynomial's.
 __device__ __forceinline__ float exp2_poly(float x) {
-    x = fmaxf(x, -127.0f);
-    const float t = x + 12582912.0f;
-    const float n = t - 12582912.0f;
+    const float n = rintf(x);
     const float f = x - n;
     float p = kP7;
     p = fmaf(p, f, kP6);
@@ -296,8 +362,7 @@ __device__ __forceinline__ float exp2_poly(float x) {
     p = fmaf(p, f, kP2);
     p = fmaf(p, f, kP1);
     p = fmaf(p, f, 1.0f);
-    const float s = __uint_as_float((__float_as_uint(t) << 23) + 0x3F800000u);
-    return p * s;
+    return p * ex2_ftz(n);
 }
 
 template <int V>
@@ -377,23 +442,23 @@ __device__ __forceinline__ void tile_f32(const float* __restrict__ sRec, int nj,
     }
 }
 
+// One work item of the FP32-compensated sweep (see f64_item).
 template <int D, int R, int V>
-__global__ void __launch_bounds__(kSweepThreads)
-sweep_f32c_kernel(SweepGeometry g, const float* __restrict__ rec,
-                  const double* __restrict__ tileMin, const double* __restrict__ tileMax,
-                  PairConsts c, double* __restrict__ partials) {
+__device__ __forceinline__ void f32c_item(const float* __restrict__ rec,
+                                          const double* __restrict__ tileMin,
+                                          const double* __restrict__ tileMax,
+                                          double* __restrict__ partials, int N, int nTiles,
+                                          int Npad, const PairConsts& c, int strip, int jt0,
+                                          int jt1, int slot, float* sRec) {
     constexpr int S = Layout<D>::kF32Stride;
-    __shared__ __align__(16) float sRec[kTile * S];
     const int tid = threadIdx.x;
-    const int strip = blockIdx.x / g.nChunks;
-    const int chunk = blockIdx.x - strip * g.nChunks;
     const int stripBase = strip * kSweepThreads * R;
 
     float xh[R][D], xl[R][D], th[R], tl[R];
     int rk[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-        const int i = min(stripBase + r * kSweepThreads + tid, g.N - 1);
+        const int i = min(stripBase + r * kSweepThreads + tid, N - 1);
         const float* ri = rec + (size_t)i * S;
 #pragma unroll
         for (int k = 0; k < D; ++k) {
@@ -408,7 +473,7 @@ sweep_f32c_kernel(SweepGeometry g, const float* __restrict__ rec,
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int tt = stripBase / kTile + r;
-        if (tt < g.nTiles) {
+        if (tt < nTiles) {
             tminI = fmin(tminI, tileMin[tt]);
             tmaxI = fmax(tmaxI, tileMax[tt]);
         }
@@ -419,13 +484,11 @@ sweep_f32c_kernel(SweepGeometry g, const float* __restrict__ rec,
 #pragma unroll
         for (int q = 0; q < kNumAcc; ++q) acc[r][q] = 0.0;
 
-    const int jt0 = chunk * g.chunkTiles;
-    const int jt1 = min(jt0 + g.chunkTiles, g.nTiles);
     for (int jt = jt0; jt < jt1; ++jt) {
         const TileMode m = tile_mode(tminI, tmaxI, tileMin[jt], tileMax[jt], c);
         if (!m.doB && !m.doS) continue;
         const int j0 = jt * kTile;
-        const int nj = min(kTile, g.N - j0);
+        const int nj = min(kTile, N - j0);
         __syncthreads();
         const float4* src = reinterpret_cast<const float4*>(rec + (size_t)j0 * S);
         float4* dst = reinterpret_cast<float4*>(sRec);
@@ -448,11 +511,30 @@ sweep_f32c_kernel(SweepGeometry g, const float* __restrict__ rec,
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int i = stripBase + r * kSweepThreads + tid;
-        if (i < g.N) {
+        if (i < N) {
 #pragma unroll
             for (int q = 0; q < kNumAcc; ++q)
-                partials[((size_t)chunk * kNumAcc + q) * g.Npad + i] = acc[r][q];
+                partials[((size_t)slot * kNumAcc + q) * Npad + i] = acc[r][q];
         }
+    }
+}
+
+template <int D, int R, int V>
+__global__ void __launch_bounds__(kSweepThreads)
+sweep_f32c_list_kernel(const SweepProblem* __restrict__ problems,
+                       const WorkItem* __restrict__ items, const int* __restrict__ nItems,
+                       int* __restrict__ counter) {
+    __shared__ __align__(16) float sRec[kTile * Layout<D>::kF32Stride];
+    __shared__ int sNext;
+    const int n = *nItems;
+    for (;;) {
+        const int it = next_item(counter, &sNext);
+        if (it >= n) break;
+        const WorkItem w = items[it];
+        const SweepProblem& P = problems[w.problem];
+        const PairConsts c = P.c;
+        f32c_item<D, R, V>(static_cast<const float*>(P.rec), P.tileMin, P.tileMax, P.partials,
+                           P.N, P.nTiles, P.Npad, c, w.strip, w.jt0, w.jt1, w.slot, sRec);
     }
 }
 
@@ -483,6 +565,32 @@ __device__ __forceinline__ void block_sum(double (&v)[NV]) {
 
 __device__ __forceinline__ double std_normal_cdf(double v) { return 0.5 * erfc(-v * kSqrtHalf); }
 
+// Per-event finish in FP64 from the six unit pair sums s (already rescaled):
+// v[0] = log lambda_i + compensator (src/NewHawkes.hpp:652-655), v[1..6] =
+// the event's gradient contributions, *prob = P_i (src/NewHawkes.hpp:685).
+__device__ __forceinline__ void event_contributions(const FinishConsts& f,
+                                                    const double (&s)[kNumAcc], double ti,
+                                                    double (&v)[8], double* prob) {
+    const double SB = f.prefB * s[0];
+    const double SS = f.prefS * s[3];
+    const double lam = SB + SS;
+    const double inv = 1.0 / lam;
+    const double Di = f.T - ti;
+    const double eW = exp(-f.omega * Di);
+    const double cdf = std_normal_cdf(f.b * Di) - std_normal_cdf(-f.b * ti);
+    v[0] = log(lam) + f.theta * (eW - 1.0) - f.mu0 * cdf;
+    v[1] = ((double)f.D / f.sigma * SS - f.sigma * f.prefS * s[4]) * inv;
+    v[2] = ((double)f.D / f.a * SB - f.a * f.prefB * s[1]) * inv;
+    const double bD = f.b * Di, bt = f.b * ti;
+    const double phiD = kInvSqrt2Pi * exp(-0.5 * bD * bD);
+    const double phiT = kInvSqrt2Pi * exp(-0.5 * bt * bt);
+    v[3] = (SB / f.b - f.b * f.prefB * s[2]) * inv - f.mu0 * (phiD * Di + phiT * ti);
+    v[4] = (SS / f.omega - f.prefS * s[5]) * inv - f.theta * Di * eW;
+    v[5] = f.seScale * s[3] * inv + (eW - 1.0);
+    v[6] = f.bgScale * s[0] * inv - cdf;
+    if (prob) *prob = SS * inv;
+}
+
 __global__ void __launch_bounds__(kFinishThreads)
 finish_kernel(SweepGeometry g, const double* __restrict__ partials,
               const double* __restrict__ times, FinishConsts f, double* __restrict__ blockSums,
@@ -500,25 +608,7 @@ finish_kernel(SweepGeometry g, const double* __restrict__ partials,
                 acc += partials[((size_t)ch * kNumAcc + q) * g.Npad + i];
             s[q] = acc * f.accScale[q];
         }
-        const double SB = f.prefB * s[0];
-        const double SS = f.prefS * s[3];
-        const double lam = SB + SS;
-        const double inv = 1.0 / lam;
-        const double ti = times[i];
-        const double Di = f.T - ti;
-        const double eW = exp(-f.omega * Di);
-        const double cdf = std_normal_cdf(f.b * Di) - std_normal_cdf(-f.b * ti);
-        v[0] = log(lam) + f.theta * (eW - 1.0) - f.mu0 * cdf;
-        v[1] = ((double)f.D / f.sigma * SS - f.sigma * f.prefS * s[4]) * inv;
-        v[2] = ((double)f.D / f.a * SB - f.a * f.prefB * s[1]) * inv;
-        const double bD = f.b * Di, bt = f.b * ti;
-        const double phiD = kInvSqrt2Pi * exp(-0.5 * bD * bD);
-        const double phiT = kInvSqrt2Pi * exp(-0.5 * bt * bt);
-        v[3] = (SB / f.b - f.b * f.prefB * s[2]) * inv - f.mu0 * (phiD * Di + phiT * ti);
-        v[4] = (SS / f.omega - f.prefS * s[5]) * inv - f.theta * Di * eW;
-        v[5] = f.seScale * s[3] * inv + (eW - 1.0);
-        v[6] = f.bgScale * s[0] * inv - cdf;
-        if (probs) probs[i] = SS * inv;
+        event_contributions(f, s, times[i], v, probs ? probs + i : nullptr);
     }
     block_sum<8, kFinishThreads>(v);
     if (threadIdx.x == 0) {
@@ -559,6 +649,59 @@ final_kernel(int nBlocks, const double* __restrict__ blockSums, FinishConsts f,
 #pragma unroll
         for (int q = 1; q < 7; ++q) out[q] = v[q];
         out[7] = 0.0;
+    }
+}
+
+// Finish over many problems: CTA b handles events [i0, i0 + kFinishThreads)
+// of problem blocks[b].problem; each event sums its strip's slots in order.
+__global__ void __launch_bounds__(kFinishThreads)
+finish_list_kernel(const FinishProblem* __restrict__ problems,
+                   const FinishBlock* __restrict__ blocks, double* __restrict__ blockSums) {
+    const FinishBlock fb = blocks[blockIdx.x];
+    const FinishProblem& P = problems[fb.problem];
+    const FinishConsts f = P.f;
+    const int N = P.N;
+    const int i = fb.i0 + threadIdx.x;
+    double v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = 0.0;
+    if (i < N) {
+        const int nc = P.stripChunks[i / P.stripEvents];
+        double s[kNumAcc];
+#pragma unroll
+        for (int q = 0; q < kNumAcc; ++q) {
+            double acc = 0.0;
+            for (int ch = 0; ch < nc; ++ch)
+                acc += P.partials[((size_t)ch * kNumAcc + q) * P.Npad + i];
+            s[q] = acc * f.accScale[q];
+        }
+        event_contributions(f, s, P.times[i], v, P.probs ? P.probs + i : nullptr);
+    }
+    block_sum<8, kFinishThreads>(v);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) blockSums[(size_t)blockIdx.x * 8 + q] = v[q];
+    }
+}
+
+// One CTA per problem: fixed-order sum of its finish CTAs' sums.
+__global__ void __launch_bounds__(kFinalThreads)
+final_list_kernel(const FinishProblem* __restrict__ problems, const double* __restrict__ blockSums,
+                  double* __restrict__ out) {
+    const FinishProblem& P = problems[blockIdx.x];
+    double v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = 0.0;
+    for (int b = threadIdx.x; b < P.nBlocks; b += kFinalThreads)
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v[q] += blockSums[(size_t)(P.blockBase + b) * 8 + q];
+    block_sum<8, kFinalThreads>(v);
+    if (threadIdx.x == 0) {
+        double* o = out + (size_t)blockIdx.x * 8;
+        o[0] = v[0] + P.f.constant;
+#pragma unroll
+        for (int q = 1; q < 7; ++q) o[q] = v[q];
+        o[7] = 0.0;
     }
 }
 
@@ -623,36 +766,104 @@ cudaError_t launch_sweep_f64(int D, int R, const SweepGeometry& g, const double*
     return cudaGetLastError();
 }
 
+namespace {
+
 template <int D, int R>
-static cudaError_t launch_f32c_variant(int V, int grid, const SweepGeometry& g, const float* rec,
-                                       const double* tileMin, const double* tileMax,
-                                       const PairConsts& c, double* partials, cudaStream_t s) {
-    switch (V) {
-        case 0: sweep_f32c_kernel<D, R, 0><<<grid, kSweepThreads, 0, s>>>(g, rec, tileMin, tileMax, c, partials); break;
-        case 1: sweep_f32c_kernel<D, R, 1><<<grid, kSweepThreads, 0, s>>>(g, rec, tileMin, tileMax, c, partials); break;
-        case 2: sweep_f32c_kernel<D, R, 2><<<grid, kSweepThreads, 0, s>>>(g, rec, tileMin, tileMax, c, partials); break;
-        case 3: sweep_f32c_kernel<D, R, 3><<<grid, kSweepThreads, 0, s>>>(g, rec, tileMin, tileMax, c, partials); break;
+cudaError_t sweep_list_dispatch_v(int precision, int V, int grid, const SweepProblem* problems,
+                                  const WorkItem* items, const int* nItems, int* counter,
+                                  cudaStream_t s, int* blocksPerSM) {
+    const void* fn = nullptr;
+    if (precision == 0) {
+        if (R > 2) return cudaErrorInvalidValue;
+        fn = reinterpret_cast<const void*>(&sweep_f64_list_kernel<D, (R > 2 ? 2 : R)>);
+    } else {
+        if (R < 2) return cudaErrorInvalidValue;
+        switch (V) {
+            case 0: fn = reinterpret_cast<const void*>(&sweep_f32c_list_kernel<D, (R < 2 ? 2 : R), 0>); break;
+            case 1: fn = reinterpret_cast<const void*>(&sweep_f32c_list_kernel<D, (R < 2 ? 2 : R), 1>); break;
+            case 2: fn = reinterpret_cast<const void*>(&sweep_f32c_list_kernel<D, (R < 2 ? 2 : R), 2>); break;
+            case 3: fn = reinterpret_cast<const void*>(&sweep_f32c_list_kernel<D, (R < 2 ? 2 : R), 3>); break;
+            default: return cudaErrorInvalidValue;
+        }
+    }
+    if (blocksPerSM) {
+        *blocksPerSM = 0;
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocksPerSM, fn, kSweepThreads, 0);
+    }
+    void* args[] = {(void*)&problems, (void*)&items, (void*)&nItems, (void*)&counter};
+    return cudaLaunchKernel(fn, dim3(grid), dim3(kSweepThreads), args, 0, s);
+}
+
+template <int D>
+cudaError_t sweep_list_dispatch_r(int precision, int R, int V, int grid,
+                                  const SweepProblem* problems, const WorkItem* items,
+                                  const int* nItems, int* counter, cudaStream_t s,
+                                  int* blocksPerSM) {
+    switch (R) {
+        case 1: return sweep_list_dispatch_v<D, 1>(precision, V, grid, problems, items, nItems,
+                                                   counter, s, blocksPerSM);
+        case 2: return sweep_list_dispatch_v<D, 2>(precision, V, grid, problems, items, nItems,
+                                                   counter, s, blocksPerSM);
+        case 4: return sweep_list_dispatch_v<D, 4>(precision, V, grid, problems, items, nItems,
+                                                   counter, s, blocksPerSM);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t sweep_list_dispatch(int precision, int D, int R, int V, int grid,
+                                const SweepProblem* problems, const WorkItem* items,
+                                const int* nItems, int* counter, cudaStream_t s,
+                                int* blocksPerSM) {
+    switch (D) {
+#define X(d) \
+    case d: return sweep_list_dispatch_r<d>(precision, R, V, grid, problems, items, nItems, \
+                                            counter, s, blocksPerSM);
+        HPHC_FOR_EACH_DIM(X)
+#undef X
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_sweep_list(int precision, int D, int R, int V, int grid,
+                              const SweepProblem* problems, const WorkItem* items,
+                              const int* nItems, int* counter, cudaStream_t s) {
+    if (grid < 1) return cudaErrorInvalidValue;
+    return sweep_list_dispatch(precision, D, R, V, grid, problems, items, nItems, counter, s,
+                               nullptr);
+}
+
+int sweep_list_blocks_per_sm(int precision, int D, int R, int V) {
+    int n = 0;
+    if (sweep_list_dispatch(precision, D, R, V, 1, nullptr, nullptr, nullptr, nullptr, 0, &n) !=
+        cudaSuccess)
+        return 0;
+    return n;
+}
+
+cudaError_t launch_pack_f32_jobs(int D, int nJobs, int maxN, const PackJob* jobs, cudaStream_t s) {
+    const dim3 grid((maxN + 255) / 256, nJobs);
+    switch (D) {
+#define X(d) \
+    case d: pack_f32_jobs_kernel<d><<<grid, 256, 0, s>>>(jobs); break;
+        HPHC_FOR_EACH_DIM(X)
+#undef X
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
 }
 
-cudaError_t launch_sweep_f32c(int D, int R, int V, const SweepGeometry& g, const float* rec,
-                              const double* tileMin, const double* tileMax, const PairConsts& c,
-                              double* partials, cudaStream_t s) {
-    const int grid = g.nStrips * g.nChunks;
-#define X(d)                                                                                    \
-    case d:                                                                                     \
-        if (R == 2) return launch_f32c_variant<d, 2>(V, grid, g, rec, tileMin, tileMax, c,      \
-                                                     partials, s);                              \
-        if (R == 4) return launch_f32c_variant<d, 4>(V, grid, g, rec, tileMin, tileMax, c,      \
-                                                     partials, s);                              \
-        return cudaErrorInvalidValue;
-    switch (D) {
-        HPHC_FOR_EACH_DIM(X)
-        default: return cudaErrorInvalidValue;
-    }
-#undef X
+cudaError_t launch_finish_list(int nBlocks, const FinishProblem* problems,
+                               const FinishBlock* blocks, double* blockSums, cudaStream_t s) {
+    finish_list_kernel<<<nBlocks, kFinishThreads, 0, s>>>(problems, blocks, blockSums);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_final_list(int nProblems, const FinishProblem* problems,
+                              const double* blockSums, double* out, cudaStream_t s) {
+    final_list_kernel<<<nProblems, kFinalThreads, 0, s>>>(problems, blockSums, out);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_finish(const SweepGeometry& g, const double* partials, const double* times,

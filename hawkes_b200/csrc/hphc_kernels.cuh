@@ -95,11 +95,7 @@ cudaError_t launch_tile_bounds(int N, const double* times, double* tileMin, doub
 cudaError_t launch_sweep_f64(int D, int R, const SweepGeometry& g, const double* rec,
                              const double* tileMin, const double* tileMax, const PairConsts& c,
                              double* partials, cudaStream_t s);
-// V selects the FP32 variant: bit 0 = coordinate lo parts, bit 1 = software
-// exponential (see hphc_kernels.cu).
-cudaError_t launch_sweep_f32c(int D, int R, int V, const SweepGeometry& g, const float* rec,
-                              const double* tileMin, const double* tileMax, const PairConsts& c,
-                              double* partials, cudaStream_t s);
+
 
 // Per-event finish: combines the chunk partials of each event in chunk order,
 // forms lambda_i, the log-likelihood and gradient contributions and (if probs
@@ -119,5 +115,74 @@ cudaError_t launch_ex2_bias(int n, double* blockSums, cudaStream_t s);
 
 // Number of finish CTAs for N events.
 inline int finish_blocks(int N) { return (N + kFinishThreads - 1) / kFinishThreads; }
+
+// ---- work-list execution ---------------------------------------------------
+//
+// A "problem" is one event set evaluated at one parameter vector.  One launch
+// of each stage serves any number of problems: a single evaluation, K
+// parameter vectors on one set (MCMC proposals), or many sets of uneven size.
+
+// Pair-sweep view of a problem.
+struct SweepProblem {
+    const void* rec;        // FP64 or FP32 records (FP32: scaled for this problem)
+    const double* tileMin;  // per kTile-event tile of the problem's set
+    const double* tileMax;
+    double* partials;       // [slot][6][Npad]
+    int N, nTiles, Npad, pad;
+    PairConsts c;
+};
+
+// One unit of sweep work: target strip `strip` of problem `problem` against j
+// tiles [jt0, jt1), written to partial-sum slot `slot` of that strip.  The
+// host lists items largest first; CTAs take them in that order from an atomic
+// counter, so slow and fast items balance across SMs, and every item writes
+// fixed slots, so results do not depend on which CTA ran it.
+struct WorkItem {
+    int problem, strip, jt0, jt1, slot, pad0, pad1, pad2;
+};
+
+// Finish view of a problem.
+struct FinishProblem {
+    const double* partials;   // [slot][6][Npad]
+    const int* stripChunks;   // slots used by each strip
+    const double* times;      // the set's raw times
+    double* probs;            // P_i output (may be null)
+    int N, Npad, stripEvents, blockBase;  // blockBase: first finish CTA of this problem
+    int nBlocks, pad0, pad1, pad2;
+    FinishConsts f;
+};
+
+struct FinishBlock {
+    int problem, i0;
+};
+
+// FP32 record build for one problem.
+struct PackJob {
+    const double* loc;
+    const double* times;
+    const int32_t* ranks;
+    float* rec;
+    double sX, sT;
+    int N, pad;
+};
+
+cudaError_t launch_pack_f32_jobs(int D, int nJobs, int maxN, const PackJob* jobs, cudaStream_t s);
+
+// Persistent sweep over a work list: `grid` CTAs take items from *counter
+// (which must be 0 at launch) until *nItems are taken.  precision: 0 = FP64,
+// 1 = FP32-compensated with variant V.
+cudaError_t launch_sweep_list(int precision, int D, int R, int V, int grid,
+                              const SweepProblem* problems, const WorkItem* items,
+                              const int* nItems, int* counter, cudaStream_t s);
+
+// Resident CTAs per SM of that sweep kernel (0 if the configuration is invalid).
+int sweep_list_blocks_per_sm(int precision, int D, int R, int V);
+
+cudaError_t launch_finish_list(int nBlocks, const FinishProblem* problems,
+                               const FinishBlock* blocks, double* blockSums, cudaStream_t s);
+
+// out[8p .. 8p+7] for every problem p: log-likelihood, gradient, 0.
+cudaError_t launch_final_list(int nProblems, const FinishProblem* problems,
+                              const double* blockSums, double* out, cudaStream_t s);
 
 }  // namespace hphc

@@ -215,12 +215,15 @@ class CudaHawkes:
         self._check(_lib.hphc_set_kernel_timing(self._h, int(bool(enable))), "setKernelTiming")
 
     def kernelTimes(self):
-        """(sweep ms, finish ms) of the last evaluation made with kernel timing on."""
+        """(sweep ms, finish ms, step ms) of the last evaluation made with kernel
+        timing on; the step spans table upload, record build, sweep, finish and
+        result copy on the device."""
         a = ctypes.c_float()
         b = ctypes.c_float()
-        self._check(_lib.hphc_get_kernel_times(self._h, ctypes.byref(a), ctypes.byref(b)),
-                    "kernelTimes")
-        return a.value, b.value
+        c = ctypes.c_float()
+        self._check(_lib.hphc_get_kernel_times(self._h, ctypes.byref(a), ctypes.byref(b),
+                                               ctypes.byref(c)), "kernelTimes")
+        return a.value, b.value, c.value
 
     def lastLaunchStats(self):
         """(kernel launches, background terms evaluated, self-excitation terms
@@ -230,6 +233,82 @@ class CudaHawkes:
         ns = ctypes.c_double()
         self._check(_lib.hphc_get_last_launch_stats(self._h, ctypes.byref(n), ctypes.byref(nb),
                                                     ctypes.byref(ns)), "lastLaunchStats")
+        return n.value, nb.value, ns.value
+
+
+class Multiset:
+    """Many independent event sets of uneven size, each evaluated at its own
+    parameter vector in one run (hphc_multiset_* in include/hphc.h)."""
+
+    def __init__(self, embeddingDimension: int, setSizes, flags: int = CUDA, device: int = 0):
+        sizes = (ctypes.c_int * len(setSizes))(*[int(n) for n in setSizes])
+        h = ctypes.c_void_p()
+        st = _lib.hphc_multiset_create(int(embeddingDimension), len(setSizes), sizes, int(flags),
+                                       int(device), ctypes.byref(h))
+        if st != 0:
+            raise HawkesError(st, "hphc_multiset_create: " +
+                              _lib.hphc_status_string(st).decode())
+        self._h = h
+        self.embeddingDimension = int(embeddingDimension)
+        self.setSizes = [int(n) for n in setSizes]
+
+    def _check(self, st: int, what: str) -> None:
+        if st != 0:
+            msg = (_lib.hphc_multiset_last_error(self._h).decode() or
+                   _lib.hphc_status_string(st).decode())
+            raise HawkesError(st, f"{what}: {msg}")
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            _lib.hphc_multiset_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def setData(self, set_index: int, locations, times) -> None:
+        loc = _as_f64(locations, "locations")
+        t = _as_f64(times, "times")
+        self._check(_lib.hphc_multiset_set_data(self._h, int(set_index), loc.ctypes.data_as(_dp),
+                                                loc.size, t.ctypes.data_as(_dp), t.size),
+                    "setData")
+
+    def logLikelihoodAndGradient(self, params):
+        """params: numSets x 6 -> (loglik[numSets], gradient[numSets, 6])."""
+        S = len(self.setSizes)
+        p = np.ascontiguousarray(np.asarray(params, dtype=np.float64).reshape(S, 6))
+        ll = np.zeros(S)
+        g = np.zeros((S, 6))
+        self._check(_lib.hphc_multiset_log_likelihood_and_gradient(
+            self._h, p.ctypes.data_as(_dp), ll.ctypes.data_as(_dp), g.ctypes.data_as(_dp)),
+            "logLikelihoodAndGradient")
+        return ll, g
+
+    def setKernelTiming(self, enable: bool = True) -> None:
+        self._check(_lib.hphc_multiset_set_kernel_timing(self._h, int(bool(enable))),
+                    "setKernelTiming")
+
+    def kernelTimes(self):
+        a, b, c = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
+        self._check(_lib.hphc_multiset_get_kernel_times(self._h, ctypes.byref(a),
+                                                        ctypes.byref(b), ctypes.byref(c)),
+                    "kernelTimes")
+        return a.value, b.value, c.value
+
+    def lastLaunchStats(self):
+        n, nb, ns = ctypes.c_int(), ctypes.c_double(), ctypes.c_double()
+        self._check(_lib.hphc_multiset_get_last_launch_stats(self._h, ctypes.byref(n),
+                                                             ctypes.byref(nb), ctypes.byref(ns)),
+                    "lastLaunchStats")
         return n.value, nb.value, ns.value
 
 

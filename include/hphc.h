@@ -160,10 +160,39 @@ int hphc_get_internal_dimension(hphc_engine* engine, int* out);
 /* ---- batched evaluation (no reference counterpart) ---------------------
  *
  * Evaluate K parameter vectors (K x 6, row-major) on the engine's events in
- * one launch sequence.  loglik has K entries; gradient (K x 6) may be null.
- * The engine's own parameters and cached results are not changed. */
+ * one run: one launch per stage for all K (MCMC proposals or parallel chains),
+ * replayed from a CUDA graph.  loglik has K entries; gradient (K x 6) may be
+ * null.  The engine's own parameters are not changed. */
 int hphc_batch_log_likelihood_and_gradient(hphc_engine* engine, const double* params, int K,
                                            double* loglik, double* gradient);
+
+/* ---- many event sets at once (no reference counterpart) -------------------
+ *
+ * A multiset holds numSets independent event sets of uneven sizes (for
+ * example many regions or many simulated data sets) and evaluates each at its
+ * own parameter vector in one run: one launch per stage for all sets, the
+ * sweep's work items taken largest first by persistent CTAs, the sequence
+ * replayed from a CUDA graph.  Same precision flags as hphc_create. */
+typedef struct hphc_multiset hphc_multiset;
+
+int hphc_multiset_create(int embeddingDimension, int numSets, const int* setSizes, long flags,
+                         int device, hphc_multiset** out);
+void hphc_multiset_destroy(hphc_multiset* multiset);
+const char* hphc_multiset_last_error(const hphc_multiset* multiset);
+
+/* Locations (setSizes[set] x D, row-major) and times of one set. */
+int hphc_multiset_set_data(hphc_multiset* multiset, int set, const double* locations,
+                           size_t locLength, const double* times, size_t timesLength);
+
+/* params: numSets x 6; loglik: numSets; gradient: numSets x 6 (may be null). */
+int hphc_multiset_log_likelihood_and_gradient(hphc_multiset* multiset, const double* params,
+                                              double* loglik, double* gradient);
+
+int hphc_multiset_set_kernel_timing(hphc_multiset* multiset, int enable);
+int hphc_multiset_get_kernel_times(hphc_multiset* multiset, float* sweepMs, float* finishMs,
+                                   float* stepMs);
+int hphc_multiset_get_last_launch_stats(hphc_multiset* multiset, int* kernelLaunches,
+                                        double* backgroundTerms, double* selfExciteTerms);
 
 /* ---- evaluation without allocation (no reference counterpart) -----------
  *
@@ -230,10 +259,11 @@ int hphc_get_sweep_shape(hphc_engine* engine, int* eventsPerThread, int* itemsPe
  * kernels of every later evaluation (enable != 0), on the engine's stream. */
 int hphc_set_kernel_timing(hphc_engine* engine, int enable);
 
-/* Device durations (ms) of the pair sweep and of the finish + final kernels
- * of the most recent evaluation made with kernel timing enabled.  Waits for
- * that evaluation to finish. */
-int hphc_get_kernel_times(hphc_engine* engine, float* sweepMs, float* finishMs);
+/* Device durations (ms) of the most recent evaluation made with kernel timing
+ * enabled, after it has been waited for (hphc_read_results or any
+ * synchronous call): the pair sweep, the finish + final kernels and the whole
+ * step (table upload, record build, sweep, finish, result copy). */
+int hphc_get_kernel_times(hphc_engine* engine, float* sweepMs, float* finishMs, float* stepMs);
 
 #ifdef __cplusplus
 }  /* extern "C" */

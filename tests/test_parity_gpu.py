@@ -175,7 +175,9 @@ def test_batch_equals_single_evaluations():
         for k in range(5):
             e.setParameters(P[k])
             lk, gk = e.getLogLikelihoodAndGradient()
-            assert lk == ll[k] and np.array_equal(gk, g[k])
+            # one run of 5 problems vs 5 runs: only the FP64 chunk-sum order differs
+            assert abs(lk - ll[k]) <= 1e-12 * abs(lk)
+            assert np.all(np.abs(gk - g[k]) <= 1e-12 * (np.abs(gk) + 1.0))
 
 
 def test_argument_errors_on_a_live_engine():
