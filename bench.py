@@ -50,10 +50,11 @@ SEED = 5
 L2_FLUSH_BYTES = 256 << 20
 
 # Algorithmic FP32 work per evaluated pair term (counted once per
-# instruction, FMA = 1): background term 11 (dx, dy, dt; d^2; exponent;
-# three weighted sums) + 1 ex2; self-excitation term 5 (exponent; three
-# weighted sums) + 1 ex2.
-FP32_PER_B, FP32_PER_S = 11.0, 5.0
+# instruction, FMA = 1): background exponential 11 (dx, dy, dt; d^2; exponent;
+# three weighted sums) + 1 ex2, and 3 more (the column's three weighted sums)
+# when one evaluation serves both events of a pair; self-excitation term 5
+# (exponent; three weighted sums) + 1 ex2.
+FP32_PER_B, FP32_PER_COL, FP32_PER_S = 11.0, 3.0, 5.0
 FP32_LANES_PER_SM = 128
 
 
@@ -401,6 +402,7 @@ def ours_arm(args):
         ms32, sweep32, res32 = time_device(fp32, args.steps, args.warmup, flusher(fp32))
         barrier()
     launches, nb, ns = fp32.eng.lastLaunchStats()
+    nev = fp32.eng.lastLaunchEvals()
     shape32 = fp32.eng.sweepShape() if w["kind"] != "sets" else None
     _, nb64, ns64 = fp64.eng.lastLaunchStats()
     steps64 = args.steps64 or args.steps
@@ -436,7 +438,8 @@ def ours_arm(args):
     max_mhz = float(peaks.get("sm_max_mhz", 1965.0))
     peak_inst = sm_count * FP32_LANES_PER_SM * max_mhz * 1e6 / 1e12
     sweep_mean = statistics.mean(sweep32)
-    achieved = (FP32_PER_B * nb + FP32_PER_S * ns) / (sweep_mean / 1e3) / 1e12
+    inst = FP32_PER_B * nev + FP32_PER_COL * (nb - nev) + FP32_PER_S * ns
+    achieved = inst / (sweep_mean / 1e3) / 1e12
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "sweep_traffic.json")
     if os.path.exists(tpath):
@@ -470,15 +473,18 @@ def ours_arm(args):
         "speedup_fp32c_vs_fp64": value / value64,
         "accuracy": acc,
         "terms": {"background": nb, "self_excitation": ns, "possible": 2 * pairs,
-                  "note": "pair terms the sweep evaluated; the rest are the non-causal half of "
-                          "the self-excitation sum and tile pairs whose terms are all exactly "
-                          "zero in FP32"},
+                  "background_exponentials": nev,
+                  "note": "pair terms the sweep accounted for; the rest are the non-causal half "
+                          "of the self-excitation sum and tile pairs whose terms are all exactly "
+                          "zero in FP32.  A background pair with the other event in an earlier "
+                          "tile is evaluated once (one exponential) for both events"},
         "roofline": {"bound": "fp32", "kernel": kernel,
                      "achieved": achieved, "peak": peak_inst, "unit": "Tinst/s",
                      "frac": achieved / peak_inst, "traffic": traffic,
-                     "count": "FP32-pipe instructions, FMA = 1: 11 per background term + 5 per "
-                              "self-excitation term evaluated, per sweep launch, over the mean "
-                              "CUDA-event duration of the sweep kernel",
+                     "count": "FP32-pipe instructions, FMA = 1: 11 per background exponential "
+                              "+ 3 per pair also added to the earlier event's sums + 5 per "
+                              "self-excitation term, per sweep launch, over the mean CUDA-event "
+                              "duration of the sweep kernel",
                      "peak_source": f"{sm_count} SMs x 128 FP32 lanes x {max_mhz:.0f} MHz "
                                     f"(sm_max_mhz, {peak_src})",
                      "sweep_ms": sweep_mean},

@@ -42,6 +42,7 @@ SIGNATURES = {
     "hphc_enqueue_log_likelihood_and_gradient": (ctypes.c_int, [_handle]),
     "hphc_read_results": (ctypes.c_int, [_handle, _c_double_p, _c_double_p, ctypes.c_size_t]),
     "hphc_get_last_launch_stats": (ctypes.c_int, [_handle, _c_int_p, _c_double_p, _c_double_p]),
+    "hphc_get_last_launch_evals": (ctypes.c_int, [_handle, _c_double_p]),
     "hphc_loglik_grad_fp64_static": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
                                                     ctypes.c_void_p, _c_double_p,
                                                     ctypes.c_void_p, ctypes.c_void_p]),
@@ -63,6 +64,7 @@ SIGNATURES = {
     "hphc_multiset_get_kernel_times": (ctypes.c_int, [_handle, ctypes.POINTER(ctypes.c_float),
                                                       ctypes.POINTER(ctypes.c_float),
                                                       ctypes.POINTER(ctypes.c_float)]),
+    "hphc_multiset_get_last_launch_evals": (ctypes.c_int, [_handle, _c_double_p]),
     "hphc_multiset_get_last_launch_stats": (ctypes.c_int, [_handle, _c_int_p, _c_double_p,
                                                            _c_double_p]),
 }

@@ -137,6 +137,7 @@ struct Mode {
     int precision = HPHC_PRECISION_FP64;
     int variant = 2;  // FP32 variant bits: 1 = coordinate lo parts, 2 = software exponential
     bool underflowSkip = true;
+    bool symmetric = true;  // FP32: each background pair evaluated once
 };
 
 Mode mode_from_flags(long fl) {
@@ -146,6 +147,7 @@ Mode mode_from_flags(long fl) {
     m.underflowSkip = !(fl & HPHC_FLAG_NO_UNDERFLOW_SKIP);
     m.variant = ((fl & HPHC_FLAG_FP32_SPACE_HILO) ? 1 : 0) |
                 ((fl & HPHC_FLAG_FP32_FAST_EXP) ? 0 : 2);
+    m.symmetric = m.precision != HPHC_PRECISION_FP64 && !(fl & HPHC_FLAG_FP32_ORDERED);
     return m;
 }
 
@@ -308,6 +310,7 @@ struct Runtime {
             return cuda_status(err, e, "exponential calibration");
         const int st = ex.init(D, mode.precision, mode.variant, mode.underflowSkip, device, stream,
                                ex2Fix);
+        ex.symmetric = mode.symmetric;
         if (st) err = ex.error;
         return st;
     }
@@ -706,6 +709,15 @@ int hphc_get_last_launch_stats(hphc_engine* e, int* kernelLaunches, double* back
     return HPHC_OK;
 }
 
+int hphc_get_last_launch_evals(hphc_engine* e, double* backgroundEvals) {
+    if (!e) return HPHC_ERR_INVALID_HANDLE;
+    if (!backgroundEvals) return HPHC_ERR_BAD_ARGUMENT;
+    double nb = 0.0, ns = 0.0;
+    std::vector<SetView> sets{e->set.view()};
+    e->rt.ex.count_terms(sets, &nb, &ns, backgroundEvals);
+    return HPHC_OK;
+}
+
 int hphc_set_sweep_shape(hphc_engine* e, int eventsPerThread, int itemsPerSM) {
     if (!e) return HPHC_ERR_INVALID_HANDLE;
     const bool fp64 = e->rt.mode.precision == HPHC_PRECISION_FP64;
@@ -867,6 +879,16 @@ int hphc_multiset_get_last_launch_stats(hphc_multiset* m, int* kernelLaunches,
         if (backgroundTerms) *backgroundTerms = nb;
         if (selfExciteTerms) *selfExciteTerms = ns;
     }
+    return HPHC_OK;
+}
+
+int hphc_multiset_get_last_launch_evals(hphc_multiset* m, double* backgroundEvals) {
+    if (!m) return HPHC_ERR_INVALID_HANDLE;
+    if (!backgroundEvals) return HPHC_ERR_BAD_ARGUMENT;
+    std::vector<SetView> views(m->S);
+    for (int s = 0; s < m->S; ++s) views[s] = m->sets[s].view();
+    double nb = 0.0, ns = 0.0;
+    m->rt.ex.count_terms(views, &nb, &ns, backgroundEvals);
     return HPHC_OK;
 }
 

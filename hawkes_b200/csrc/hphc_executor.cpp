@@ -102,6 +102,7 @@ void Executor::release() {
     if (hStaging_) cudaFreeHost(hStaging_);
     if (dRecPool_) cudaFree(dRecPool_);
     if (dPartials_) cudaFree(dPartials_);
+    if (dColAcc_) cudaFree(dColAcc_);
     if (dBlockSums_) cudaFree(dBlockSums_);
     if (dOut_) cudaFree(dOut_);
     if (hOut_) cudaFreeHost(hOut_);
@@ -111,8 +112,9 @@ void Executor::release() {
     dTables_ = hStaging_ = nullptr;
     dRecPool_ = nullptr;
     dPartials_ = dBlockSums_ = dOut_ = hOut_ = nullptr;
+    dColAcc_ = nullptr;
     dCounter_ = nullptr;
-    tablesCap_ = stagingCap_ = recCap_ = partialsCap_ = blockCap_ = outCap_ = 0;
+    tablesCap_ = stagingCap_ = recCap_ = partialsCap_ = blockCap_ = outCap_ = colCap_ = 0;
     for (auto& ev : ev_) ev = nullptr;
 }
 
@@ -191,7 +193,7 @@ int Executor::build_plan(const std::vector<SetView>& sets, const int* setOf, con
     const int target = numSMs_ * items;
     const int nChunksTarget = std::max(1, (int)std::ceil(target / std::max(1.0, totalStrips)));
 
-    size_t recOff = 0, partOff = 0;
+    size_t recOff = 0, partOff = 0, colOff = 0;
     std::vector<size_t> chunkBase(P);
     int blockBase = 0;
     for (int p = 0; p < P; ++p) {
@@ -222,6 +224,12 @@ int Executor::build_plan(const std::vector<SetView>& sets, const int* setOf, con
         sp.tileMax = s.dTileMax;
         sp.partials = reinterpret_cast<double*>(partOff);  // offset, fixed up later
         partOff += (size_t)maxChunks * kNumAcc * Npad;
+        sp.symmetric = (fp32 && symmetric && N <= kMaxSymmetricEvents) ? 1 : 0;
+        sp.colAcc = nullptr;
+        if (sp.symmetric) {
+            sp.colAcc = reinterpret_cast<unsigned long long*>(colOff + 1);  // offset + 1
+            colOff += (size_t)3 * Npad;
+        }
         if (fp32) {
             sp.rec = reinterpret_cast<const void*>(recOff);  // offset, fixed up later
             PackJob j{};
@@ -262,13 +270,19 @@ int Executor::build_plan(const std::vector<SetView>& sets, const int* setOf, con
                     if (needed(m)) b = m; else a = m + 1;
                 }
                 lo = std::max(0, a - 1);
-                a = ts1;
-                b = nTiles;
-                while (a < b) {
-                    const int m = (a + b) / 2;
-                    if (needed(m)) a = m + 1; else b = m;
+                if (sp.symmetric) {
+                    // pairs with later tiles are added as columns by the later
+                    // strips; sorted times leave no self-excitation there
+                    hi = ts1;
+                } else {
+                    a = ts1;
+                    b = nTiles;
+                    while (a < b) {
+                        const int m = (a + b) / 2;
+                        if (needed(m)) a = m + 1; else b = m;
+                    }
+                    hi = std::min(nTiles, a + 1);
                 }
-                hi = std::min(nTiles, a + 1);
             }
             // Chunks sit on a fixed grid of CT tiles per problem, so a tile
             // always lands in the same chunk whatever the band: skipping a
@@ -289,6 +303,7 @@ int Executor::build_plan(const std::vector<SetView>& sets, const int* setOf, con
 
         FinishProblem& fp = pl.fp[p];
         fp.partials = nullptr;  // fixed up later
+        fp.colAcc = nullptr;
         fp.stripChunks = nullptr;
         fp.times = s.dTimes;
         fp.probs = (p == 0) ? dProbs : nullptr;
@@ -320,6 +335,7 @@ int Executor::build_plan(const std::vector<SetView>& sets, const int* setOf, con
 
     recNeed_ = recOff;
     partialsNeed_ = partOff;
+    colNeed_ = colOff;
     int st = ensure_buffers();
     if (st) return st;
 
@@ -330,9 +346,11 @@ int Executor::build_plan(const std::vector<SetView>& sets, const int* setOf, con
         SweepProblem& sp = pl.sp[p];
         const size_t po = reinterpret_cast<size_t>(sp.partials);
         sp.partials = dPartials_ + po;
+        if (sp.colAcc) sp.colAcc = dColAcc_ + (reinterpret_cast<size_t>(sp.colAcc) - 1);
         if (fp32) sp.rec = dRecPool_ + reinterpret_cast<size_t>(sp.rec);
         FinishProblem& fp = pl.fp[p];
         fp.partials = sp.partials;
+        fp.colAcc = sp.colAcc;
         fp.stripChunks = reinterpret_cast<const int*>(d + offChunks_) + chunkBase[p];
     }
     for (auto& j : pl.pj) j.rec = dRecPool_ + reinterpret_cast<size_t>(j.rec);
@@ -366,6 +384,9 @@ int Executor::ensure_buffers() {
                       std::max<size_t>(recNeed_, 1) * sizeof(float))) != cudaSuccess ||
         (e = grow_dev(reinterpret_cast<void**>(&dPartials_), partialsCap_,
                       std::max<size_t>(partialsNeed_, 1) * sizeof(double))) != cudaSuccess ||
+        (e = grow_dev(reinterpret_cast<void**>(&dColAcc_), colCap_,
+                      std::max<size_t>(colNeed_, 1) * sizeof(unsigned long long))) !=
+            cudaSuccess ||
         (e = grow_dev(reinterpret_cast<void**>(&dBlockSums_), blockCap_,
                       (size_t)std::max(pl.nBlocks, 1) * 8 * sizeof(double))) != cudaSuccess ||
         (e = grow_dev(&dTables_, tablesCap_, tablesBytes_)) != cudaSuccess)
@@ -425,6 +446,9 @@ int Executor::launch_sequence(int grid) {
     }
     if ((e = cudaMemsetAsync(dCounter_, 0, sizeof(int), stream_)))
         return cuda_fail(e, "reset work counter");
+    if (colNeed_ && (e = cudaMemsetAsync(dColAcc_, 0, colNeed_ * sizeof(unsigned long long),
+                                         stream_)))
+        return cuda_fail(e, "reset column sums");
     if (kernelTiming && (e = record(ev_[1]))) return cuda_fail(e, "timing event");
     if ((e = launch_sweep_list(prec, D_, R, variant_, grid, sp, items, nItems, dCounter_, stream_)))
         return cuda_fail(e, "sweep kernel");
@@ -446,7 +470,8 @@ int Executor::autotune(const std::vector<SetView>& sets, const int* setOf, const
                        int P, double* dProbs) {
     double pairs = 0.0;
     for (int p = 0; p < P; ++p) pairs += (double)sets[setOf[p]].N * sets[setOf[p]].N;
-    const auto key = std::make_tuple(D_, precision_, variant_, log2_bucket(pairs), log2_bucket(P));
+    const auto key = std::make_tuple(D_, precision_, variant_ | (symmetric ? 16 : 0),
+                                     log2_bucket(pairs), log2_bucket(P));
     {
         std::lock_guard<std::mutex> lock(gTuneMutex);
         auto it = gTuneCache.find(key);
@@ -474,18 +499,20 @@ int Executor::autotune(const std::vector<SetView>& sets, const int* setOf, const
             itemsPerSM = it;
             if ((st = build_plan(sets, setOf, params, P, dProbs, r, it))) break;
             const int grid = sweep_grid(r);
-            for (int rep = 0; rep < 2 && !st; ++rep) st = launch_sequence(grid);
+            // best of three sweeps (the first also warms the caches)
+            float ms = 1e30f;
+            for (int rep = 0; rep < 3 && !st; ++rep) {
+                if ((st = launch_sequence(grid))) break;
+                cudaError_t e = cudaStreamSynchronize(stream_);
+                float t = 0.f;
+                if (e == cudaSuccess) e = cudaEventElapsedTime(&t, ev_[1], ev_[2]);
+                if (e != cudaSuccess) {
+                    st = cuda_fail(e, "autotune timing");
+                    break;
+                }
+                ms = std::min(ms, t);
+            }
             if (st) break;
-            cudaError_t e = cudaStreamSynchronize(stream_);
-            if (e != cudaSuccess) {
-                st = cuda_fail(e, "autotune");
-                break;
-            }
-            float ms = 0.f;
-            if ((e = cudaEventElapsedTime(&ms, ev_[1], ev_[2])) != cudaSuccess) {
-                st = cuda_fail(e, "autotune timing");
-                break;
-            }
             if (ms < best) {
                 best = ms;
                 bestR = r;
@@ -537,11 +564,13 @@ int Executor::enqueue(const std::vector<SetView>& sets, const int* setOf, const 
     key.R = R;
     key.grid = grid;
     key.tablesBytes = tablesBytes_;
+    key.colNeed = colNeed_;
     key.tables = dTables_;
     key.timing = kernelTiming;
     const bool same = graphExec_ && key.P == graphKey_.P && key.nBlocks == graphKey_.nBlocks &&
                       key.maxN == graphKey_.maxN && key.R == graphKey_.R &&
                       key.grid == graphKey_.grid && key.tablesBytes == graphKey_.tablesBytes &&
+                      key.colNeed == graphKey_.colNeed &&
                       key.tables == graphKey_.tables && key.timing == graphKey_.timing;
     cudaError_t e;
     if (!same) {
@@ -588,9 +617,9 @@ int Executor::wait(double* hostOut) {
     return HPHC_OK;
 }
 
-void Executor::count_terms(const std::vector<SetView>& sets, double* bTerms,
-                           double* sTerms) const {
-    double nb = 0.0, ns = 0.0;
+void Executor::count_terms(const std::vector<SetView>& sets, double* bTerms, double* sTerms,
+                           double* bEvals) const {
+    double nb = 0.0, ns = 0.0, ne = 0.0;
     const int stripEvents = kSweepThreads * R;
     for (const WorkItem& w : plan_.items) {
         const SetView& s = sets[plan_.setOf[w.problem]];
@@ -603,16 +632,23 @@ void Executor::count_terms(const std::vector<SetView>& sets, double* bTerms,
             tmaxI = std::max(tmaxI, s.hTileMax[t]);
         }
         const double ni = std::min(stripEvents, s.N - w.strip * stripEvents);
+        const bool sym = plan_.sp[w.problem].symmetric != 0;
         for (int jt = w.jt0; jt < w.jt1; ++jt) {
             bool b, se;
             tile_needs(tminI, tmaxI, s.hTileMin[jt], s.hTileMax[jt], c, &b, &se);
+            if (sym && jt >= ts1) b = false;
             const double nj = std::min(kTile, s.N - jt * kTile);
-            if (b) nb += ni * nj;
+            if (b) {
+                // a symmetric tile also accounts for the pairs' other order
+                nb += (sym && jt < ts0 ? 2.0 : 1.0) * ni * nj;
+                ne += ni * nj;
+            }
             if (se) ns += ni * nj;
         }
     }
     *bTerms = nb;
     *sTerms = ns;
+    if (bEvals) *bEvals = ne;
 }
 
 }  // namespace hphc

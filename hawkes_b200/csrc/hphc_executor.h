@@ -42,8 +42,9 @@ struct SetView {
 
 struct RunStats {
     int launches = 0;        // kernels launched by the last run
-    double bTerms = 0.0;     // background pair terms the sweep evaluated
+    double bTerms = 0.0;     // background pair terms the sweep accounted for
     double sTerms = 0.0;     // self-excitation pair terms the sweep evaluated
+    double bEvals = 0.0;     // background exponentials evaluated (a symmetric pair: one)
 };
 
 class Executor {
@@ -62,14 +63,18 @@ public:
     // gradient, 0) to hostOut.
     int wait(double* hostOut);
 
-    // Pair terms the last run's sweep evaluated (replays the tile decisions).
-    void count_terms(const std::vector<SetView>& sets, double* bTerms, double* sTerms) const;
+    // Pair terms the last run's sweep accounted for (replays the tile
+    // decisions): background terms (both orders of a symmetric pair),
+    // self-excitation terms, and background exponentials evaluated.
+    void count_terms(const std::vector<SetView>& sets, double* bTerms, double* sTerms,
+                     double* bEvals = nullptr) const;
 
     std::string error;
     int fixedR = 0, fixedItems = 0;  // sweep shape overrides; 0 = autotune
     int R = 2, itemsPerSM = 16;      // shape in use
     bool useGraph = true;
     bool kernelTiming = false;
+    bool symmetric = false;  // FP32: symmetric background sweep (set before the first enqueue)
     float lastSweepMs = 0.f, lastFinishMs = 0.f, lastStepMs = 0.f;
     bool timedValid = false;
     int lastLaunches = 0;
@@ -102,6 +107,8 @@ private:
     size_t recCap_ = 0;
     double* dPartials_ = nullptr;
     size_t partialsCap_ = 0;
+    unsigned long long* dColAcc_ = nullptr;
+    size_t colCap_ = 0;
     double* dBlockSums_ = nullptr;
     size_t blockCap_ = 0;
     double* dOut_ = nullptr;
@@ -115,12 +122,13 @@ private:
            offPJ_ = 0, tablesBytes_ = 0;
     size_t itemsCap_ = 0;
     size_t recNeed_ = 0, partialsNeed_ = 0;  // floats / doubles the last plan needs
+    size_t colNeed_ = 0;                     // column-sum words the last plan needs
 
     // graph
     cudaGraphExec_t graphExec_ = nullptr;
     struct GraphKey {
         int P = -1, nBlocks = -1, maxN = -1, R = -1, grid = -1;
-        size_t tablesBytes = 0;
+        size_t tablesBytes = 0, colNeed = 0;
         void* tables = nullptr;
         bool timing = false;
     } graphKey_;

@@ -442,23 +442,167 @@ __device__ __forceinline__ void tile_f32(const float* __restrict__ sRec, int nj,
     }
 }
 
+// ---- symmetric background tiles ----
+//
+// For a tile J before the strip, each pair (i, j) is evaluated once and its
+// background terms B, B d'^2, B dt'^2 go to row i (registers, as above) and
+// to column j.  Column sums are formed per warp in groups of 8 columns: lane
+// l visits the group's columns in the order jj ^ (l >> 2), so that after the
+// loop register cp[jj] of lane l holds column (jj ^ (l >> 2)) summed over the
+// lane's R rows; a transposing exchange (shuffles at distances 16, 8, 4 that
+// each keep the half of the columns the lane ends with, then 2 and 1) leaves
+// lane l with the warp total of column l >> 2, with no selects.  The 4 warp
+// totals of a column are added in FP64 in warp order and added to the
+// column's fixed-point sum, so the result does not depend on CTA order.
+
+constexpr int kSymGroup = 8;  // columns per warp exchange
+
+template <int D, int R, int V, bool DO_S, bool MASK>
+__device__ __forceinline__ void sym_group_f32(const float* __restrict__ sRec, int g, int perm,
+                                              const float (&xh)[R][D], const float (&xl)[R][D],
+                                              const float (&th)[R], const float (&tl)[R],
+                                              const int (&rk)[R], const PairConsts& c,
+                                              float (&a)[R][kNumAcc],
+                                              float (&cp)[kSymGroup][3]) {
+    constexpr int S = Layout<D>::kF32Stride;
+#pragma unroll
+    for (int jj = 0; jj < kSymGroup; ++jj) {
+        const int j = g + (jj ^ perm);
+        float rj[S];
+#pragma unroll
+        for (int v = 0; v < S / 4; ++v) {
+            const float4 q = reinterpret_cast<const float4*>(sRec + j * S)[v];
+            rj[4 * v] = q.x;
+            rj[4 * v + 1] = q.y;
+            rj[4 * v + 2] = q.z;
+            rj[4 * v + 3] = q.w;
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            float d2 = 0.0f;
+#pragma unroll
+            for (int k = 0; k < D; ++k) {
+                const float dd = (V & kSpaceLo) ? (xh[r][k] - rj[k]) + (xl[r][k] - rj[D + 1 + k])
+                                                : xh[r][k] - rj[k];
+                d2 = fmaf(dd, dd, d2);
+            }
+            const float dt = (th[r] - rj[D]) + (tl[r] - rj[2 * D + 1]);
+            const float t2 = dt * dt;
+            const float e = (V & kPolyExp) ? -(d2 + t2) : (c.ex2Fix - d2) - t2;
+            const float B = exp2_term<V>(e);
+            a[r][0] += B;
+            a[r][1] = fmaf(B, d2, a[r][1]);
+            a[r][2] = fmaf(B, t2, a[r][2]);
+            if (r == 0) {
+                cp[jj][0] = B;
+                cp[jj][1] = B * d2;
+                cp[jj][2] = B * t2;
+            } else {
+                cp[jj][0] += B;
+                cp[jj][1] = fmaf(B, d2, cp[jj][1]);
+                cp[jj][2] = fmaf(B, t2, cp[jj][2]);
+            }
+            if (DO_S) {
+                const float es = fminf(
+                    fmaf(c.fSh, d2, fmaf(c.fWh, dt, fmaf(c.fSl, d2, fmaf(c.fWl, dt, c.ex2Fix)))),
+                    127.0f);
+                float Sv = exp2_term<V>(es);
+                if (MASK) Sv = rk[r] > __float_as_int(rj[2 * D + 2]) ? Sv : 0.0f;
+                a[r][3] += Sv;
+                a[r][4] = fmaf(Sv, d2, a[r][4]);
+                a[r][5] = fmaf(Sv, dt, a[r][5]);
+            }
+        }
+    }
+}
+
+// Warp total of column (lane >> 2) of the group from the permuted partials.
+__device__ __forceinline__ float sym_exchange(const float (&cp)[kSymGroup][3], int q) {
+    constexpr unsigned kAll = 0xffffffffu;
+    const float u0 = cp[0][q] + __shfl_xor_sync(kAll, cp[4][q], 16);
+    const float u1 = cp[1][q] + __shfl_xor_sync(kAll, cp[5][q], 16);
+    const float u2 = cp[2][q] + __shfl_xor_sync(kAll, cp[6][q], 16);
+    const float u3 = cp[3][q] + __shfl_xor_sync(kAll, cp[7][q], 16);
+    const float w0 = u0 + __shfl_xor_sync(kAll, u2, 8);
+    const float w1 = u1 + __shfl_xor_sync(kAll, u3, 8);
+    float x = w0 + __shfl_xor_sync(kAll, w1, 4);
+    x += __shfl_xor_sync(kAll, x, 2);
+    x += __shfl_xor_sync(kAll, x, 1);
+    return x;
+}
+
+// One full tile J (kTile columns, all real events) before the strip.
+// sCol: [kSweepThreads / 32][3][kTile] floats of shared memory.
+template <int D, int R, int V, bool DO_S, bool MASK>
+__device__ __forceinline__ void tile_sym_f32(const float* __restrict__ sRec,
+                                             const float (&xh)[R][D], const float (&xl)[R][D],
+                                             const float (&th)[R], const float (&tl)[R],
+                                             const int (&rk)[R], const PairConsts& c,
+                                             double (&acc)[R][kNumAcc], float* __restrict__ sCol,
+                                             unsigned long long* __restrict__ colAcc, int Npad,
+                                             int j0) {
+    static_assert(kSweepThreads == kTile, "one column per thread in the column flush");
+    static_assert(kFlush % kSymGroup == 0 && kTile % kFlush == 0, "group sizes");
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int perm = lane >> 2;
+    for (int jb = 0; jb < kTile; jb += kFlush) {
+        float a[R][kNumAcc];
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+#pragma unroll
+            for (int q = 0; q < kNumAcc; ++q) a[r][q] = 0.0f;
+#pragma unroll 1
+        for (int g = jb; g < jb + kFlush; g += kSymGroup) {
+            float cp[kSymGroup][3];
+            sym_group_f32<D, R, V, DO_S, MASK>(sRec, g, perm, xh, xl, th, tl, rk, c, a, cp);
+            const float c0 = sym_exchange(cp, 0);
+            const float c1 = sym_exchange(cp, 1);
+            const float c2 = sym_exchange(cp, 2);
+            if ((lane & 3) == 0) {
+                float* o = sCol + warp * 3 * kTile + g + perm;
+                o[0] = c0;
+                o[kTile] = c1;
+                o[2 * kTile] = c2;
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+#pragma unroll
+            for (int q = 0; q < kNumAcc; ++q) acc[r][q] += (double)a[r][q];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        double v = 0.0;
+#pragma unroll
+        for (int w = 0; w < kSweepThreads / 32; ++w) v += (double)sCol[(w * 3 + q) * kTile + tid];
+        atomicAdd(colAcc + (size_t)q * Npad + j0 + tid,
+                  (unsigned long long)__double2ll_rn(v * kColScale));
+    }
+}
+
 // One work item of the FP32-compensated sweep (see f64_item).
 template <int D, int R, int V>
 __device__ __forceinline__ void f32c_item(const float* __restrict__ rec,
                                           const double* __restrict__ tileMin,
                                           const double* __restrict__ tileMax,
-                                          double* __restrict__ partials, int N, int nTiles,
-                                          int Npad, const PairConsts& c, int strip, int jt0,
-                                          int jt1, int slot, float* sRec) {
+                                          double* __restrict__ partials,
+                                          unsigned long long* __restrict__ colAcc, int N,
+                                          int nTiles, int Npad, bool sym, const PairConsts& c,
+                                          int strip, int jt0, int jt1, int slot, float* sRec,
+                                          float* sCol) {
     constexpr int S = Layout<D>::kF32Stride;
     const int tid = threadIdx.x;
     const int stripBase = strip * kSweepThreads * R;
+    const int ts0 = stripBase / kTile, ts1 = min(ts0 + R, nTiles);
 
     float xh[R][D], xl[R][D], th[R], tl[R];
     int rk[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-        const int i = min(stripBase + r * kSweepThreads + tid, N - 1);
+        const int iRaw = stripBase + r * kSweepThreads + tid;
+        const int i = min(iRaw, N - 1);
         const float* ri = rec + (size_t)i * S;
 #pragma unroll
         for (int k = 0; k < D; ++k) {
@@ -468,6 +612,13 @@ __device__ __forceinline__ void f32c_item(const float* __restrict__ rec,
         th[r] = ri[D];
         tl[r] = ri[2 * D + 1];
         rk[r] = __float_as_int(ri[2 * D + 2]);
+        if (iRaw >= N) {
+            // Padding rows of the last strip: a time 1e18 away makes every
+            // background term exactly +0 (exponent ~ -1e36, finite), so they
+            // add nothing to the column sums; their own rows are discarded.
+            th[r] = 1e18f;
+            tl[r] = 0.0f;
+        }
     }
     double tminI = INFINITY, tmaxI = -INFINITY;
 #pragma unroll
@@ -485,7 +636,8 @@ __device__ __forceinline__ void f32c_item(const float* __restrict__ rec,
         for (int q = 0; q < kNumAcc; ++q) acc[r][q] = 0.0;
 
     for (int jt = jt0; jt < jt1; ++jt) {
-        const TileMode m = tile_mode(tminI, tmaxI, tileMin[jt], tileMax[jt], c);
+        TileMode m = tile_mode(tminI, tmaxI, tileMin[jt], tileMax[jt], c);
+        if (sym && jt >= ts1) m.doB = false;  // covered as columns by later strips
         if (!m.doB && !m.doS) continue;
         const int j0 = jt * kTile;
         const int nj = min(kTile, N - j0);
@@ -494,7 +646,18 @@ __device__ __forceinline__ void f32c_item(const float* __restrict__ rec,
         float4* dst = reinterpret_cast<float4*>(sRec);
         for (int v = tid; v < nj * (S / 4); v += kSweepThreads) dst[v] = src[v];
         __syncthreads();
-        if (m.doB) {
+        if (sym && m.doB && jt < ts0) {
+            // jt < ts0 <= nTiles - 1: a full tile
+            if (!m.doS)
+                tile_sym_f32<D, R, V, false, false>(sRec, xh, xl, th, tl, rk, c, acc, sCol,
+                                                    colAcc, Npad, j0);
+            else if (m.allCausal)
+                tile_sym_f32<D, R, V, true, false>(sRec, xh, xl, th, tl, rk, c, acc, sCol, colAcc,
+                                                   Npad, j0);
+            else
+                tile_sym_f32<D, R, V, true, true>(sRec, xh, xl, th, tl, rk, c, acc, sCol, colAcc,
+                                                  Npad, j0);
+        } else if (m.doB) {
             if (!m.doS)
                 tile_f32<D, R, V, true, false, false>(sRec, nj, xh, xl, th, tl, rk, c, acc);
             else if (m.allCausal)
@@ -519,12 +682,15 @@ __device__ __forceinline__ void f32c_item(const float* __restrict__ rec,
     }
 }
 
+// R = 2 fits 128 registers (4 CTAs per SM); R = 4 holds twice the rows and
+// column partials and runs 2 CTAs per SM.
 template <int D, int R, int V>
-__global__ void __launch_bounds__(kSweepThreads)
+__global__ void __launch_bounds__(kSweepThreads, (R <= 2 ? 4 : 2))
 sweep_f32c_list_kernel(const SweepProblem* __restrict__ problems,
                        const WorkItem* __restrict__ items, const int* __restrict__ nItems,
                        int* __restrict__ counter) {
     __shared__ __align__(16) float sRec[kTile * Layout<D>::kF32Stride];
+    __shared__ __align__(16) float sCol[(kSweepThreads / 32) * 3 * kTile];
     __shared__ int sNext;
     const int n = *nItems;
     for (;;) {
@@ -534,7 +700,8 @@ sweep_f32c_list_kernel(const SweepProblem* __restrict__ problems,
         const SweepProblem& P = problems[w.problem];
         const PairConsts c = P.c;
         f32c_item<D, R, V>(static_cast<const float*>(P.rec), P.tileMin, P.tileMax, P.partials,
-                           P.N, P.nTiles, P.Npad, c, w.strip, w.jt0, w.jt1, w.slot, sRec);
+                           P.colAcc, P.N, P.nTiles, P.Npad, P.symmetric != 0, c, w.strip, w.jt0,
+                           w.jt1, w.slot, sRec, sCol);
     }
 }
 
@@ -673,6 +840,7 @@ finish_list_kernel(const FinishProblem* __restrict__ problems,
             double acc = 0.0;
             for (int ch = 0; ch < nc; ++ch)
                 acc += P.partials[((size_t)ch * kNumAcc + q) * P.Npad + i];
+            if (q < 3 && P.colAcc) acc += (double)P.colAcc[(size_t)q * P.Npad + i] * kColInv;
             s[q] = acc * f.accScale[q];
         }
         event_contributions(f, s, P.times[i], v, P.probs ? P.probs + i : nullptr);

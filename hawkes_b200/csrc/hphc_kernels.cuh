@@ -122,13 +122,29 @@ inline int finish_blocks(int N) { return (N + kFinishThreads - 1) / kFinishThrea
 // of each stage serves any number of problems: a single evaluation, K
 // parameter vectors on one set (MCMC proposals), or many sets of uneven size.
 
+// Fixed-point scale of the column sums of the symmetric sweep (2^36): the
+// sums are non-negative and below 2^27 (at most N terms of at most 1), so
+// they fit an unsigned 64-bit integer, and integer addition makes them
+// independent of the order in which CTAs add to them.
+constexpr double kColScale = 68719476736.0;
+constexpr double kColInv = 1.0 / 68719476736.0;
+constexpr int kMaxSymmetricEvents = 1 << 27;
+
 // Pair-sweep view of a problem.
+//
+// Symmetric sweeps (FP32 records): the background kernel B_ij is symmetric,
+// so a strip of targets i evaluates each pair with an earlier tile once and
+// adds it to both its own rows and, as fixed-point column sums in colAcc, to
+// the rows of the earlier tile; pairs inside the strip's own tiles are
+// evaluated in both orders, and tiles after the strip carry only
+// self-excitation terms (zero for sorted times).
 struct SweepProblem {
     const void* rec;        // FP64 or FP32 records (FP32: scaled for this problem)
     const double* tileMin;  // per kTile-event tile of the problem's set
     const double* tileMax;
     double* partials;       // [slot][6][Npad]
-    int N, nTiles, Npad, pad;
+    unsigned long long* colAcc;  // [3][Npad] background column sums x kColScale, or null
+    int N, nTiles, Npad, symmetric;
     PairConsts c;
 };
 
@@ -144,6 +160,7 @@ struct WorkItem {
 // Finish view of a problem.
 struct FinishProblem {
     const double* partials;   // [slot][6][Npad]
+    const unsigned long long* colAcc;  // [3][Npad] symmetric-sweep column sums, or null
     const int* stripChunks;   // slots used by each strip
     const double* times;      // the set's raw times
     double* probs;            // P_i output (may be null)

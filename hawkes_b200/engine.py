@@ -46,6 +46,7 @@ COMPENSATED = 1 << 9
 NO_UNDERFLOW_SKIP = 1 << 10
 FP32_FAST_EXP = 1 << 11
 FP32_SPACE_HILO = 1 << 12
+FP32_ORDERED = 1 << 13
 
 PRECISION_FP64 = 0
 PRECISION_FP32_COMP = 1
@@ -235,6 +236,13 @@ class CudaHawkes:
                                                     ctypes.byref(ns)), "lastLaunchStats")
         return n.value, nb.value, ns.value
 
+    def lastLaunchEvals(self):
+        """Background exponentials the last evaluation computed (a pair
+        evaluated once for both of its events counts once)."""
+        v = ctypes.c_double()
+        self._check(_lib.hphc_get_last_launch_evals(self._h, ctypes.byref(v)), "lastLaunchEvals")
+        return v.value
+
 
 class Multiset:
     """Many independent event sets of uneven size, each evaluated at its own
@@ -310,6 +318,12 @@ class Multiset:
                                                              ctypes.byref(nb), ctypes.byref(ns)),
                     "lastLaunchStats")
         return n.value, nb.value, ns.value
+
+    def lastLaunchEvals(self):
+        v = ctypes.c_double()
+        self._check(_lib.hphc_multiset_get_last_launch_evals(self._h, ctypes.byref(v)),
+                    "lastLaunchEvals")
+        return v.value
 
 
 def factory(embeddingDimension: int, locationCount: int, flags: int, device: int = 0,

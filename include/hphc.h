@@ -69,6 +69,9 @@ extern "C" {
                                                 components lose accuracy (~1e-6) */
 #define HPHC_FLAG_FP32_SPACE_HILO (1L << 12) /* coordinate differences from hi/lo float
                                                 pairs (times always use hi/lo pairs) */
+#define HPHC_FLAG_FP32_ORDERED (1L << 13)    /* evaluate both orders of every background
+                                                pair (by default each pair is evaluated
+                                                once and added to both events' sums) */
 
 /* Precision modes reported by hphc_get_precision(). */
 #define HPHC_PRECISION_FP64 0          /* plain FP64 pair terms and reductions           */
@@ -193,6 +196,7 @@ int hphc_multiset_get_kernel_times(hphc_multiset* multiset, float* sweepMs, floa
                                    float* stepMs);
 int hphc_multiset_get_last_launch_stats(hphc_multiset* multiset, int* kernelLaunches,
                                         double* backgroundTerms, double* selfExciteTerms);
+int hphc_multiset_get_last_launch_evals(hphc_multiset* multiset, double* backgroundEvals);
 
 /* ---- evaluation without allocation (no reference counterpart) -----------
  *
@@ -246,6 +250,12 @@ int hphc_read_results(hphc_engine* engine, double* loglik, double* gradient, siz
  * terms all underflow to exactly zero in the working precision. */
 int hphc_get_last_launch_stats(hphc_engine* engine, int* kernelLaunches,
                                double* backgroundTerms, double* selfExciteTerms);
+
+/* Background exponentials the most recent evaluation's sweep computed.  In the
+ * FP32-compensated mode each background pair (i, j) with j in a tile before
+ * i's strip is evaluated once and counted once, but stands for two terms in
+ * backgroundTerms above (B_ij in event i's sum, B_ji in event j's). */
+int hphc_get_last_launch_evals(hphc_engine* engine, double* backgroundEvals);
 
 /* Sweep shape: target events per thread (2 or 4; a CTA strip holds 128 times
  * as many) and the number of (strip, j-range) work items per SM the j range is

@@ -26,11 +26,13 @@ pytestmark = pytest.mark.gpu
 FP64 = hb.CUDA
 FP32C = hb.CUDA | hb.COMPENSATED
 FP32F = hb.CUDA | hb.COMPENSATED | hb.FP32_FAST_EXP
+FP32O = hb.CUDA | hb.COMPENSATED | hb.FP32_ORDERED
 TOL = {FP64: dict(ll=1e-10, grad=1e-10, probs=1e-10),
        FP32C: dict(ll=1e-7, grad=5e-6, probs=2e-5),
-       FP32F: dict(ll=1e-7, grad=5e-6, probs=2e-5)}
-MODES = [FP64, FP32C, FP32F]
-IDS = ["fp64", "fp32c", "fp32c_fast"]
+       FP32F: dict(ll=1e-7, grad=5e-6, probs=2e-5),
+       FP32O: dict(ll=1e-7, grad=5e-6, probs=2e-5)}
+MODES = [FP64, FP32C, FP32F, FP32O]
+IDS = ["fp64", "fp32c", "fp32c_fast", "fp32c_ordered"]
 
 
 def engine(loc, t, p, flags):
@@ -100,6 +102,46 @@ def test_random_cases_against_oracle(flags):
 
 
 @pytest.mark.parametrize("flags", MODES, ids=IDS)
+def test_unsorted_times_against_oracle(flags):
+    # Times in no particular order (the last one is the largest, so T bounds
+    # them): every tile pair may hold self-excitation terms in either order.
+    rng = np.random.default_rng(77)
+    for N, D in ((1000, 2), (700, 3)):
+        loc = rng.uniform(0, 10, size=(N, D))
+        t = rng.uniform(0, 500, size=N)
+        k = int(np.argmax(t))
+        t[[k, N - 1]] = t[[N - 1, k]]
+        t[: N // 3] = np.sort(t[: N // 3])  # partly sorted, partly not
+        p = workloads.BASE_PARAMS * np.array([1.0, 1.0, 3.0, 1.0, 1.0, 1.0])
+        o = oracle.oracle_eval(loc, t, p, threads=8)
+        c = {"loc": loc, "t": t, "params": p, "ref_loglik": o["loglik"],
+             "ref_probs": o["probs"], "oracle_grad": o["grad"], "grad_scale": o["grad_scale"],
+             "grad_term_scale": o["grad_term_scale"]}
+        check_case(f"unsorted_D{D}_N{N}", c, flags)
+
+
+def test_symmetric_sweep_halves_background_work():
+    # Each background pair with an earlier tile is evaluated once for both
+    # events: the same terms are accounted for with about half the exponentials.
+    loc, t = workloads.uniform(30000, seed=21)
+    p = workloads.BASE_PARAMS
+    with engine(loc, t, p, FP32C) as s, engine(loc, t, p, FP32O) as o:
+        for e in (s, o):
+            e.setSweepShape(2, 16)
+        ls, gs = s.getLogLikelihoodAndGradient()
+        lo, go = o.getLogLikelihoodAndGradient()
+        _, nbs, nss = s.lastLaunchStats()
+        _, nbo, nso = o.lastLaunchStats()
+        evs, evo = s.lastLaunchEvals(), o.lastLaunchEvals()
+    # The tile-level skip is decided per (strip, tile); a pair's other order
+    # is decided from the other event's strip, so the two modes may account
+    # for slightly different sets of exactly-zero terms.
+    assert abs(nbs - nbo) <= 0.01 * nbo and nss == nso
+    assert evo == nbo and evs < 0.55 * evo
+    assert abs(ls - lo) <= 1e-9 * abs(lo)
+
+
+@pytest.mark.parametrize("flags", MODES, ids=IDS)
 def test_underflow_skip_is_bit_exact(flags):
     # Tile pairs whose terms all underflow are skipped; evaluating them anyway
     # must give identical bits.
@@ -118,7 +160,7 @@ def test_underflow_skip_is_bit_exact(flags):
     assert nbb == 20000.0 ** 2  # without it every background term is evaluated
 
 
-@pytest.mark.parametrize("flags", [FP64, FP32C], ids=["fp64", "fp32c"])
+@pytest.mark.parametrize("flags", [FP64, FP32C, FP32O], ids=["fp64", "fp32c", "fp32c_ordered"])
 def test_repeatable_bits(flags):
     loc, t = workloads.uniform(5000, seed=8)
     with engine(loc, t, workloads.BASE_PARAMS, flags) as e:
