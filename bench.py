@@ -49,13 +49,22 @@ N_EVENTS = 100000
 SEED = 5
 L2_FLUSH_BYTES = 256 << 20
 
-# Algorithmic FP32 work per evaluated pair term (counted once per
-# instruction, FMA = 1): background exponential 11 (dx, dy, dt; d^2; exponent;
-# three weighted sums) + 1 ex2, and 3 more (the column's three weighted sums)
-# when one evaluation serves both events of a pair; self-excitation term 5
-# (exponent; three weighted sums) + 1 ex2.
+# Algorithmic work of the brute-force pair sum (FMA = 1 instruction): every
+# ordered pair (i, j) has a background term, 11 FP32 instructions (dx, dy, dt;
+# d^2; exponent; three weighted sums) + 1 ex2; the causal half has a
+# self-excitation term, 5 FP32 (exponent; three weighted sums) + 1 ex2.  Per
+# pair-eval: 11 + 5/2 = 13.5 FP32 instructions and 1.5 ex2.  The roofline
+# counts this per-pair figure times the N^2 pair-evals one sweep launch
+# stands for, so it credits the tile-level skips (non-causal half, exact
+# underflow, one exponential for both orders of a background pair) as work
+# done; "evaluated" below counts only the terms the launch computed.
+FP32_PER_PAIR_EVAL, EX2_PER_PAIR_EVAL = 13.5, 1.5
+# Per evaluated term: background exponential 11, plus 3 (the column's three
+# weighted sums) when one evaluation serves both events of a pair;
+# self-excitation term 5.
 FP32_PER_B, FP32_PER_COL, FP32_PER_S = 11.0, 3.0, 5.0
 FP32_LANES_PER_SM = 128
+MUFU_LANES_PER_SM = 16
 
 
 def env_int(name, default):
@@ -437,9 +446,12 @@ def ours_arm(args):
     sm_count = torch.cuda.get_device_properties(local).multi_processor_count
     max_mhz = float(peaks.get("sm_max_mhz", 1965.0))
     peak_inst = sm_count * FP32_LANES_PER_SM * max_mhz * 1e6 / 1e12
+    peak_ex2 = sm_count * MUFU_LANES_PER_SM * max_mhz * 1e6 / 1e12
     sweep_mean = statistics.mean(sweep32)
+    achieved = FP32_PER_PAIR_EVAL * pairs / (sweep_mean / 1e3) / 1e12
+    achieved_ex2 = EX2_PER_PAIR_EVAL * pairs / (sweep_mean / 1e3) / 1e12
     inst = FP32_PER_B * nev + FP32_PER_COL * (nb - nev) + FP32_PER_S * ns
-    achieved = inst / (sweep_mean / 1e3) / 1e12
+    achieved_eval = inst / (sweep_mean / 1e3) / 1e12
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "sweep_traffic.json")
     if os.path.exists(tpath):
@@ -481,12 +493,21 @@ def ours_arm(args):
         "roofline": {"bound": "fp32", "kernel": kernel,
                      "achieved": achieved, "peak": peak_inst, "unit": "Tinst/s",
                      "frac": achieved / peak_inst, "traffic": traffic,
-                     "count": "FP32-pipe instructions, FMA = 1: 11 per background exponential "
-                              "+ 3 per pair also added to the earlier event's sums + 5 per "
-                              "self-excitation term, per sweep launch, over the mean CUDA-event "
-                              "duration of the sweep kernel",
+                     "count": f"{FP32_PER_PAIR_EVAL} FP32 instructions (FMA = 1) per pair-eval "
+                              "(11 background on every ordered pair + 5 self-excitation on the "
+                              f"causal half) x {pairs:.4g} pair-evals per sweep launch, over the "
+                              "mean CUDA-event duration of the sweep kernel",
                      "peak_source": f"{sm_count} SMs x 128 FP32 lanes x {max_mhz:.0f} MHz "
                                     f"(sm_max_mhz, {peak_src})",
+                     "ex2": {"achieved": achieved_ex2, "peak": peak_ex2, "unit": "Tex2/s",
+                             "frac": achieved_ex2 / peak_ex2,
+                             "count": f"{EX2_PER_PAIR_EVAL} ex2 per pair-eval; peak {sm_count} "
+                                      f"SMs x 16 MUFU lanes x {max_mhz:.0f} MHz"},
+                     "evaluated": {"achieved": achieved_eval, "frac": achieved_eval / peak_inst,
+                                   "count": "only the terms this launch computed: 11 per "
+                                            "background exponential + 3 per pair also added to "
+                                            "the earlier event's sums + 5 per self-excitation "
+                                            "term"},
                      "sweep_ms": sweep_mean},
         "e2e": {"value": world * pairs / e2e_s, "unit": UNIT,
                 "h2d_bytes_per_step": w["h2d"], "d2h_bytes_per_step": w["d2h"]},

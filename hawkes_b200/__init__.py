@@ -5,14 +5,16 @@ the C ABI in include/hphc.h); this package is its Python host interface.
 """
 from .engine import (  # noqa: F401
     AVX, AVX512, COMPENSATED, CUDA, FLOAT, FP32_FAST_EXP, FP32_ORDERED, FP32_SPACE_HILO,
-    NO_UNDERFLOW_SKIP,
-    OPENCL, PARAMETER_NAMES,
+    NO_INCREMENTAL, NO_UNDERFLOW_SKIP,
+    OPENCL, PARAMETER_NAMES, PATH_INCREMENTAL, PATH_KEPT_SUMS, PATH_SWEEP,
     PRECISION_FP32_COMP, PRECISION_FP64, SSE, TBB, CudaHawkes, Engine, HawkesError, Multiset,
     createEngine, engineInitial, factory, getGradient, getLogLikelihood, getProbsSelfExcite,
     setParameters, setTimesData, updateLocations)
+from .sampler import Potential, Sampler, log_prior, sampler  # noqa: F401
 
 __all__ = [
     "CudaHawkes", "Engine", "HawkesError", "Multiset", "factory", "createEngine", "engineInitial",
     "updateLocations", "setTimesData", "setParameters", "getLogLikelihood",
-    "getProbsSelfExcite", "getGradient", "PARAMETER_NAMES",
+    "getProbsSelfExcite", "getGradient", "PARAMETER_NAMES", "Sampler", "sampler", "Potential",
+    "log_prior",
 ]

@@ -43,6 +43,7 @@ SIGNATURES = {
     "hphc_read_results": (ctypes.c_int, [_handle, _c_double_p, _c_double_p, ctypes.c_size_t]),
     "hphc_get_last_launch_stats": (ctypes.c_int, [_handle, _c_int_p, _c_double_p, _c_double_p]),
     "hphc_get_last_launch_evals": (ctypes.c_int, [_handle, _c_double_p]),
+    "hphc_get_last_evaluation_path": (ctypes.c_int, [_handle, _c_int_p]),
     "hphc_loglik_grad_fp64_static": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
                                                     ctypes.c_void_p, _c_double_p,
                                                     ctypes.c_void_p, ctypes.c_void_p]),
@@ -67,7 +68,24 @@ SIGNATURES = {
     "hphc_multiset_get_last_launch_evals": (ctypes.c_int, [_handle, _c_double_p]),
     "hphc_multiset_get_last_launch_stats": (ctypes.c_int, [_handle, _c_int_p, _c_double_p,
                                                            _c_double_p]),
+    "hphc_sampler_create": (ctypes.c_int, [ctypes.c_int, _c_double_p, ctypes.c_double,
+                                           ctypes.c_int, ctypes.c_ulonglong,
+                                           ctypes.POINTER(ctypes.c_void_p)]),
+    "hphc_sampler_destroy": (None, [_handle]),
+    "hphc_sampler_last_error": (ctypes.c_char_p, [_handle]),
+    "hphc_sampler_run": (ctypes.c_int, [_handle, _handle, ctypes.c_int, ctypes.c_int, _c_double_p,
+                                        _c_double_p]),
+    "hphc_sampler_run_with": (ctypes.c_int, [_handle, ctypes.c_void_p, ctypes.c_void_p,
+                                             ctypes.c_int, ctypes.c_int, _c_double_p,
+                                             _c_double_p]),
+    "hphc_sampler_get_state": (ctypes.c_int, [_handle, _c_double_p, _c_double_p, _c_double_p,
+                                              ctypes.POINTER(ctypes.c_longlong),
+                                              ctypes.POINTER(ctypes.c_longlong)]),
 }
+
+# Signature of hphc_batch_loglik_fn (a batched log-likelihood evaluator).
+BATCH_LOGLIK_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, _c_double_p, ctypes.c_int,
+                                   _c_double_p)
 
 
 def _load() -> ctypes.CDLL:

@@ -353,6 +353,38 @@ struct hphc_engine {
     bool dirty = true;
     int lastLaunches = 0;
 
+    // Incremental evaluation.  After an evaluation of the engine's own
+    // parameters, dSums keeps every event's six unit pair sums (natural
+    // units, [6][N]) for sumsParams.  Moving a few events (updateLocations
+    // with an index) records their previous locations; the next evaluation at
+    // the same parameters updates the sums in O(N) per moved event and
+    // re-runs only the O(N) finish, instead of the O(N^2) sweep.  storeState
+    // keeps a device copy of the sums, which restoreState brings back.
+    bool incremental = true;
+    DevBuf<double> dSums, dStoredSums, dRowPartials, dIncBlockSums, dIncOut;
+    HostBuf<double> hIncOut;
+    bool sumsValid = false, storedSumsValid = false, recStale = false;
+    double sumsParams[6] = {0, 0, 0, 0, 0, 0}, storedSumsParams[6] = {0, 0, 0, 0, 0, 0};
+    double pendingSumsParams[6] = {0, 0, 0, 0, 0, 0};
+    bool pendingSums = false;
+    std::vector<int> moved;            // moved events, in order of their first move
+    std::vector<double> movedOld;      // their locations when the sums were formed (D each)
+    std::vector<int> movedSlot;        // event -> index into moved, or -1
+    int maxMoved = 1;
+    int lastPath = HPHC_PATH_SWEEP;
+    double lastIncTerms = 0.0;  // pair terms of the last incremental evaluation
+
+    void clear_moved() {
+        for (int k : moved) movedSlot[k] = -1;
+        moved.clear();
+        movedOld.clear();
+    }
+
+    void invalidate_sums() {
+        sumsValid = false;
+        clear_moved();
+    }
+
     int fail(int status, const char* f, ...) {
         char buf[512];
         va_list ap;
@@ -378,6 +410,18 @@ struct hphc_engine {
         std::memset(hLoc[1].p, 0, nl * sizeof(double));
         if ((e = set.alloc(D, N, rt.mode.precision)) || (e = dProbs.reserve(N)))
             return cuda_status(lastError, e, "device allocation");
+        incremental = !(fl & HPHC_FLAG_NO_INCREMENTAL);
+        if (incremental) {
+            if ((e = dSums.reserve((size_t)kNumAcc * N)) ||
+                (e = dStoredSums.reserve((size_t)kNumAcc * N)) ||
+                (e = dRowPartials.reserve((size_t)kNumAcc * move_event_blocks(N))) ||
+                (e = dIncBlockSums.reserve((size_t)8 * finish_blocks(N))) ||
+                (e = dIncOut.reserve(8)) || (e = hIncOut.reserve(8)))
+                return cuda_status(lastError, e, "device allocation");
+            movedSlot.assign(N, -1);
+            const int nTiles = (N + kTile - 1) / kTile;
+            maxMoved = std::max(1, std::min(64, nTiles / 4));
+        }
         set.derive_times();
         dirty = true;
         return HPHC_OK;
@@ -390,6 +434,12 @@ struct hphc_engine {
         hLoc[1].release();
         set.release();
         dProbs.release();
+        dSums.release();
+        dStoredSums.release();
+        dRowPartials.release();
+        dIncBlockSums.release();
+        dIncOut.release();
+        hIncOut.release();
     }
 
     int upload_if_dirty() {
@@ -398,18 +448,35 @@ struct hphc_engine {
                                          &lastLaunches);
         if (e != cudaSuccess) return cuda_status(lastError, e, "upload");
         dirty = false;
+        recStale = false;  // the upload re-packs the records
         return HPHC_OK;
     }
 
-    // Enqueue K parameter vectors on this engine's events.
+    // Enqueue K parameter vectors on this engine's events (full sweep).
     int enqueue(const double* p, int K, bool wantProbs) {
         lastLaunches = 0;
+        lastPath = HPHC_PATH_SWEEP;
+        // moved events are only on the host, and after incremental row uploads
+        // the packed FP64 records are stale: upload and pack everything (the
+        // kept sums and the moved list stay a consistent pair)
+        if (!moved.empty() || recStale) dirty = true;
         int st = upload_if_dirty();
         if (st) return st;
         std::vector<SetView> sets{set.view()};
         std::vector<int> setOf(K, 0);
+        // a single evaluation keeps its sums for later incremental updates
+        pendingSums = incremental && K == 1;
+        rt.ex.sumsOut = pendingSums ? dSums.p : nullptr;
+        if (pendingSums) {
+            invalidate_sums();
+            std::memcpy(pendingSumsParams, p, sizeof pendingSumsParams);
+        }
         st = rt.ex.enqueue(sets, setOf.data(), p, K, wantProbs ? dProbs.p : nullptr);
-        if (st) return fmt(lastError, st, "%s", rt.ex.error.c_str());
+        rt.ex.sumsOut = nullptr;
+        if (st) {
+            pendingSums = false;
+            return fmt(lastError, st, "%s", rt.ex.error.c_str());
+        }
         lastLaunches += rt.ex.lastLaunches;
         return HPHC_OK;
     }
@@ -417,13 +484,74 @@ struct hphc_engine {
     int wait(int K) {
         hOut.resize((size_t)K * 8);
         const int st = rt.ex.wait(hOut.data());
-        if (st) return fmt(lastError, st, "%s", rt.ex.error.c_str());
+        if (st) {
+            pendingSums = false;
+            return fmt(lastError, st, "%s", rt.ex.error.c_str());
+        }
+        if (pendingSums) {
+            sumsValid = true;
+            std::memcpy(sumsParams, pendingSumsParams, sizeof sumsParams);
+            pendingSums = false;
+        }
+        return HPHC_OK;
+    }
+
+    bool can_update(const double* p) const {
+        return incremental && sumsValid && !pendingSums &&
+               std::memcmp(p, sumsParams, sizeof sumsParams) == 0;
+    }
+
+    // O(N) evaluation from the kept sums: upload and apply each moved event,
+    // then the per-event finish.
+    int evaluate_incremental(const double* p, double* loglik, double* grad, double* probs) {
+        lastLaunches = 0;
+        const bool hadMoves = !moved.empty();
+        const bool wasDirty = dirty;
+        int st = upload_if_dirty();
+        if (st) return st;
+        cudaStream_t s = rt.stream;
+        const PairConsts c = rt.ex.pair_consts(p);
+        cudaError_t e = cudaSuccess;
+        for (size_t m = 0; m < moved.size(); ++m) {
+            MovedEvent mv{};
+            mv.k = moved[m];
+            for (int a = 0; a < D; ++a) mv.oldLoc[a] = movedOld[m * D + a];
+            const size_t off = (size_t)mv.k * D;
+            if (!wasDirty &&
+                (e = cudaMemcpyAsync(set.dLoc.p + off, hLoc[curLoc].p + off, D * sizeof(double),
+                                     cudaMemcpyHostToDevice, s)))
+                return cuda_status(lastError, e, "upload moved event");
+            if ((e = launch_move_event(D, N, mv, set.dLoc.p, set.dTimes.p, c, dSums.p,
+                                       dRowPartials.p, s)) ||
+                (e = launch_move_event_row(N, mv.k, dRowPartials.p, dSums.p, s)))
+                return cuda_status(lastError, e, "move event");
+            lastLaunches += 2;
+        }
+        if (hadMoves && !wasDirty && rt.mode.precision == HPHC_PRECISION_FP64) recStale = true;
+        lastIncTerms = (double)moved.size() * (3.0 * N - 2.0);
+        clear_moved();
+        const FinishConsts f = rt.ex.finish_consts(p, set.view());
+        if ((e = launch_finish_sums(N, dSums.p, set.dTimes.p, f, dIncBlockSums.p,
+                                    probs ? dProbs.p : nullptr, dIncOut.p, s)) ||
+            (e = cudaMemcpyAsync(hIncOut.p, dIncOut.p, 8 * sizeof(double),
+                                 cudaMemcpyDeviceToHost, s)))
+            return cuda_status(lastError, e, "finish from kept sums");
+        lastLaunches += 2;
+        if ((e = cudaStreamSynchronize(s))) return cuda_status(lastError, e, "evaluation");
+        if (probs &&
+            (e = cudaMemcpy(probs, dProbs.p, (size_t)N * sizeof(double), cudaMemcpyDeviceToHost)))
+            return cuda_status(lastError, e, "read probabilities");
+        if (loglik) *loglik = hIncOut.p[0];
+        if (grad)
+            for (int k = 0; k < 6; ++k) grad[k] = hIncOut.p[1 + k];
+        lastPath = hadMoves ? HPHC_PATH_INCREMENTAL : HPHC_PATH_KEPT_SUMS;
         return HPHC_OK;
     }
 
     int evaluate(const double* p, double* loglik, double* grad, double* probs) {
         DeviceGuard g(rt.device);
         if (!g.ok) return fail(HPHC_ERR_CUDA, "cannot select device %d", rt.device);
+        if (can_update(p)) return evaluate_incremental(p, loglik, grad, probs);
         int st = enqueue(p, 1, probs != nullptr);
         if (st) return st;
         if ((st = wait(1))) return st;
@@ -539,6 +667,7 @@ int hphc_set_times_data(hphc_engine* e, const double* data, size_t length) {
     std::memcpy(e->set.hTimes.p, data, length * sizeof(double));
     e->set.derive_times();
     e->dirty = true;
+    e->invalidate_sums();
     return HPHC_OK;
 }
 
@@ -562,8 +691,24 @@ int hphc_update_locations(hphc_engine* e, int locationIndex, const double* locat
     size_t bad = 0;
     if (!all_finite(location, length, &bad))
         return e->fail(HPHC_ERR_NONFINITE, "locations: entry %zu is not finite", bad);
-    std::memcpy(e->hLoc[e->curLoc].p + offset, location, length * sizeof(double));
-    e->dirty = true;
+    double* row = e->hLoc[e->curLoc].p + offset;
+    if (locationIndex >= 0 && e->sumsValid) {
+        // one event moves: keep the location its sums were formed with
+        if (e->movedSlot[locationIndex] < 0) {
+            if ((int)e->moved.size() >= e->maxMoved) {
+                e->invalidate_sums();  // cheaper to sweep again
+                e->dirty = true;
+            } else {
+                e->movedSlot[locationIndex] = (int)e->moved.size();
+                e->moved.push_back(locationIndex);
+                e->movedOld.insert(e->movedOld.end(), row, row + e->D);
+            }
+        }
+    } else {
+        e->invalidate_sums();
+        e->dirty = true;
+    }
+    std::memcpy(row, location, length * sizeof(double));
     return HPHC_OK;
 }
 
@@ -618,6 +763,17 @@ int hphc_store_state(hphc_engine* e) {
     std::memcpy(e->storedParams, e->params, sizeof e->params);
     std::memcpy(e->hLoc[1 - e->curLoc].p, e->hLoc[e->curLoc].p,
                 (size_t)e->N * e->D * sizeof(double));
+    // the kept sums describe the stored locations when no event has moved since
+    e->storedSumsValid = false;
+    if (e->sumsValid && e->moved.empty()) {
+        DeviceGuard g(e->rt.device);
+        const cudaError_t err = cudaMemcpyAsync(e->dStoredSums.p, e->dSums.p,
+                                                (size_t)kNumAcc * e->N * sizeof(double),
+                                                cudaMemcpyDeviceToDevice, e->rt.stream);
+        if (err != cudaSuccess) return cuda_status(e->lastError, err, "store sums");
+        e->storedSumsValid = true;
+        std::memcpy(e->storedSumsParams, e->sumsParams, sizeof e->sumsParams);
+    }
     return HPHC_OK;
 }
 
@@ -627,6 +783,15 @@ int hphc_restore_state(hphc_engine* e) {
     std::memcpy(e->params, e->storedParams, sizeof e->params);
     e->curLoc = 1 - e->curLoc;
     e->dirty = true;
+    e->clear_moved();
+    if (e->storedSumsValid) {
+        std::swap(e->dSums, e->dStoredSums);
+        std::memcpy(e->sumsParams, e->storedSumsParams, sizeof e->sumsParams);
+        e->sumsValid = true;
+        e->storedSumsValid = false;
+    } else {
+        e->sumsValid = false;
+    }
     return HPHC_OK;
 }
 
@@ -695,10 +860,24 @@ int hphc_read_results(hphc_engine* e, double* loglik, double* gradient, size_t l
     return HPHC_OK;
 }
 
+int hphc_get_last_evaluation_path(hphc_engine* e, int* path) {
+    if (!e) return HPHC_ERR_INVALID_HANDLE;
+    if (!path) return e->fail(HPHC_ERR_BAD_ARGUMENT, "null output");
+    *path = e->lastPath;
+    return HPHC_OK;
+}
+
 int hphc_get_last_launch_stats(hphc_engine* e, int* kernelLaunches, double* backgroundTerms,
                                double* selfExciteTerms) {
     if (!e) return HPHC_ERR_INVALID_HANDLE;
     if (kernelLaunches) *kernelLaunches = e->lastLaunches;
+    if (e->lastPath != HPHC_PATH_SWEEP) {
+        // per moved event: its pair with every other event at the old and the
+        // new location, and its new row
+        if (backgroundTerms) *backgroundTerms = e->lastIncTerms;
+        if (selfExciteTerms) *selfExciteTerms = e->lastIncTerms;
+        return HPHC_OK;
+    }
     if (backgroundTerms || selfExciteTerms) {
         double nb = 0.0, ns = 0.0;
         std::vector<SetView> sets{e->set.view()};
@@ -712,6 +891,10 @@ int hphc_get_last_launch_stats(hphc_engine* e, int* kernelLaunches, double* back
 int hphc_get_last_launch_evals(hphc_engine* e, double* backgroundEvals) {
     if (!e) return HPHC_ERR_INVALID_HANDLE;
     if (!backgroundEvals) return HPHC_ERR_BAD_ARGUMENT;
+    if (e->lastPath != HPHC_PATH_SWEEP) {
+        *backgroundEvals = e->lastIncTerms;
+        return HPHC_OK;
+    }
     double nb = 0.0, ns = 0.0;
     std::vector<SetView> sets{e->set.view()};
     e->rt.ex.count_terms(sets, &nb, &ns, backgroundEvals);

@@ -307,6 +307,7 @@ int Executor::build_plan(const std::vector<SetView>& sets, const int* setOf, con
         fp.stripChunks = nullptr;
         fp.times = s.dTimes;
         fp.probs = (p == 0) ? dProbs : nullptr;
+        fp.sums = (p == 0) ? sumsOut : nullptr;
         fp.N = N;
         fp.Npad = Npad;
         fp.stripEvents = stripEvents;

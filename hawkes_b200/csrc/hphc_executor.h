@@ -75,6 +75,7 @@ public:
     bool useGraph = true;
     bool kernelTiming = false;
     bool symmetric = false;  // FP32: symmetric background sweep (set before the first enqueue)
+    double* sumsOut = nullptr;  // if set, problem 0's unit pair sums ([6][N], natural units)
     float lastSweepMs = 0.f, lastFinishMs = 0.f, lastStepMs = 0.f;
     bool timedValid = false;
     int lastLaunches = 0;

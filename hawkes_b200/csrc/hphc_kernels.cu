@@ -842,6 +842,7 @@ finish_list_kernel(const FinishProblem* __restrict__ problems,
                 acc += P.partials[((size_t)ch * kNumAcc + q) * P.Npad + i];
             if (q < 3 && P.colAcc) acc += (double)P.colAcc[(size_t)q * P.Npad + i] * kColInv;
             s[q] = acc * f.accScale[q];
+            if (P.sums) P.sums[(size_t)q * N + i] = s[q];
         }
         event_contributions(f, s, P.times[i], v, P.probs ? P.probs + i : nullptr);
     }
@@ -870,6 +871,102 @@ final_list_kernel(const FinishProblem* __restrict__ problems, const double* __re
 #pragma unroll
         for (int q = 1; q < 7; ++q) o[q] = v[q];
         o[7] = 0.0;
+    }
+}
+
+// ------------------------------------------------------- incremental --
+
+constexpr int kMoveThreads = 256;
+
+// Unit pair terms of target i against source j in natural units (FP64): the
+// background weights exp(cA d^2 + cB dt^2) x {1, d^2, dt^2} and, for dt > 0,
+// the self-excitation weights exp(cS d^2 + cW dt) x {1, d^2, dt}.
+__device__ __forceinline__ void unit_terms(double d2, double dt, const PairConsts& c,
+                                           double (&u)[kNumAcc]) {
+    const double t2 = dt * dt;
+    const double B = exp(fma(c.cA, d2, c.cB * t2));
+    u[0] = B;
+    u[1] = B * d2;
+    u[2] = B * t2;
+    const double S = dt > 0.0 ? exp(fma(c.cS, d2, c.cW * dt)) : 0.0;
+    u[3] = S;
+    u[4] = S * d2;
+    u[5] = S * dt;
+}
+
+template <int D>
+__global__ void __launch_bounds__(kMoveThreads)
+move_event_kernel(int N, MovedEvent m, const double* __restrict__ loc,
+                  const double* __restrict__ times, PairConsts c, double* __restrict__ sums,
+                  double* __restrict__ rowPartials) {
+    const int i = blockIdx.x * kMoveThreads + threadIdx.x;
+    const int k = m.k;
+    double row[kNumAcc];
+#pragma unroll
+    for (int q = 0; q < kNumAcc; ++q) row[q] = 0.0;
+    if (i < N) {
+        const double ti = times[i], tk = times[k];
+        double d2New = 0.0, d2Old = 0.0;
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+            const double xi = loc[(size_t)i * D + a];
+            const double dn = xi - loc[(size_t)k * D + a];
+            const double dOld = xi - m.oldLoc[a];
+            d2New = fma(dn, dn, d2New);
+            d2Old = fma(dOld, dOld, d2Old);
+        }
+        if (i != k) {
+            // event i's sums: its pair with k moves from the old to the new location
+            double un[kNumAcc], uo[kNumAcc];
+            unit_terms(d2New, ti - tk, c, un);
+            unit_terms(d2Old, ti - tk, c, uo);
+#pragma unroll
+            for (int q = 0; q < kNumAcc; ++q) sums[(size_t)q * N + i] += un[q] - uo[q];
+        }
+        // event k's new row: its pair with i (i == k: the j = i background term)
+        unit_terms(d2New, tk - ti, c, row);
+    }
+    double v[kNumAcc];
+#pragma unroll
+    for (int q = 0; q < kNumAcc; ++q) v[q] = row[q];
+    block_sum<kNumAcc, kMoveThreads>(v);
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int q = 0; q < kNumAcc; ++q) rowPartials[(size_t)blockIdx.x * kNumAcc + q] = v[q];
+}
+
+__global__ void __launch_bounds__(kFinalThreads)
+move_event_row_kernel(int N, int k, int nBlocks, const double* __restrict__ rowPartials,
+                      double* __restrict__ sums) {
+    double v[kNumAcc];
+#pragma unroll
+    for (int q = 0; q < kNumAcc; ++q) v[q] = 0.0;
+    for (int b = threadIdx.x; b < nBlocks; b += kFinalThreads)
+#pragma unroll
+        for (int q = 0; q < kNumAcc; ++q) v[q] += rowPartials[(size_t)b * kNumAcc + q];
+    block_sum<kNumAcc, kFinalThreads>(v);
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int q = 0; q < kNumAcc; ++q) sums[(size_t)q * N + k] = v[q];
+}
+
+__global__ void __launch_bounds__(kFinishThreads)
+finish_sums_kernel(int N, const double* __restrict__ sums, const double* __restrict__ times,
+                   FinishConsts f, double* __restrict__ blockSums, double* __restrict__ probs) {
+    const int i = blockIdx.x * kFinishThreads + threadIdx.x;
+    double v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = 0.0;
+    if (i < N) {
+        double s[kNumAcc];
+#pragma unroll
+        for (int q = 0; q < kNumAcc; ++q) s[q] = sums[(size_t)q * N + i];
+        event_contributions(f, s, times[i], v, probs ? probs + i : nullptr);
+    }
+    block_sum<8, kFinishThreads>(v);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) blockSums[(size_t)blockIdx.x * 8 + q] = v[q];
     }
 }
 
@@ -1051,6 +1148,41 @@ cudaError_t launch_ex2_bias(int n, double* blockSums, cudaStream_t s) {
 cudaError_t launch_final(int nBlocks, const double* blockSums, const FinishConsts& f, double* out,
                          cudaStream_t s) {
     final_kernel<<<1, kFinalThreads, 0, s>>>(nBlocks, blockSums, f, out);
+    return cudaGetLastError();
+}
+
+int move_event_blocks(int N) { return (N + kMoveThreads - 1) / kMoveThreads; }
+
+cudaError_t launch_move_event(int D, int N, const MovedEvent& m, const double* loc,
+                              const double* times, const PairConsts& c, double* sums,
+                              double* rowPartials, cudaStream_t s) {
+    const int blocks = move_event_blocks(N);
+    switch (D) {
+#define X(d)                                                                                     \
+    case d:                                                                                      \
+        move_event_kernel<d><<<blocks, kMoveThreads, 0, s>>>(N, m, loc, times, c, sums,          \
+                                                              rowPartials);                      \
+        break;
+        HPHC_FOR_EACH_DIM(X)
+#undef X
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_move_event_row(int N, int k, const double* rowPartials, double* sums,
+                                  cudaStream_t s) {
+    move_event_row_kernel<<<1, kFinalThreads, 0, s>>>(N, k, move_event_blocks(N), rowPartials,
+                                                      sums);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_finish_sums(int N, const double* sums, const double* times,
+                               const FinishConsts& f, double* blockSums, double* probs,
+                               double* out, cudaStream_t s) {
+    finish_sums_kernel<<<finish_blocks(N), kFinishThreads, 0, s>>>(N, sums, times, f, blockSums,
+                                                                   probs);
+    final_kernel<<<1, kFinalThreads, 0, s>>>(finish_blocks(N), blockSums, f, out);
     return cudaGetLastError();
 }
 

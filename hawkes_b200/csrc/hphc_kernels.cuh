@@ -164,6 +164,7 @@ struct FinishProblem {
     const int* stripChunks;   // slots used by each strip
     const double* times;      // the set's raw times
     double* probs;            // P_i output (may be null)
+    double* sums;             // [6][N] unit pair sums out, natural units (may be null)
     int N, Npad, stripEvents, blockBase;  // blockBase: first finish CTA of this problem
     int nBlocks, pad0, pad1, pad2;
     FinishConsts f;
@@ -201,5 +202,37 @@ cudaError_t launch_finish_list(int nBlocks, const FinishProblem* problems,
 // out[8p .. 8p+7] for every problem p: log-likelihood, gradient, 0.
 cudaError_t launch_final_list(int nProblems, const FinishProblem* problems,
                               const double* blockSums, double* out, cudaStream_t s);
+
+// ---- incremental evaluation ------------------------------------------------
+//
+// After an evaluation the engine can keep each event's six unit pair sums
+// (natural units, FP64, [6][N]).  When one event k moves and the parameters
+// are unchanged, every other event's sums change only by its pair with k, and
+// k's own sums are one O(N) row: the update is O(N) instead of the O(N^2)
+// sweep.
+
+struct MovedEvent {
+    double oldLoc[kMaxDim];  // the location the sums were computed with
+    int k;                   // event index
+    int pad;
+};
+
+// sums[q][i] += u_q(i, k at its new location) - u_q(i, k at oldLoc) for every
+// i != k (one thread per event, FP64), and per-CTA partial sums of event k's
+// new row over all j (rowPartials[cta][6]).  loc: N x D raw coordinates
+// (event k already at its new location), times: N raw times.
+cudaError_t launch_move_event(int D, int N, const MovedEvent& m, const double* loc,
+                              const double* times, const PairConsts& c, double* sums,
+                              double* rowPartials, cudaStream_t s);
+// sums[q][k] = fixed-order sum of the launch's row partials.
+cudaError_t launch_move_event_row(int N, int k, const double* rowPartials, double* sums,
+                                  cudaStream_t s);
+// Per-event finish from kept sums (natural units) and the fixed-order total:
+// out[0] = log-likelihood, out[1..6] = gradient, out[7] = 0; probs may be null.
+cudaError_t launch_finish_sums(int N, const double* sums, const double* times,
+                               const FinishConsts& f, double* blockSums, double* probs,
+                               double* out, cudaStream_t s);
+// CTAs of launch_move_event for N events.
+int move_event_blocks(int N);
 
 }  // namespace hphc

@@ -47,6 +47,12 @@ NO_UNDERFLOW_SKIP = 1 << 10
 FP32_FAST_EXP = 1 << 11
 FP32_SPACE_HILO = 1 << 12
 FP32_ORDERED = 1 << 13
+NO_INCREMENTAL = 1 << 14
+
+# How an evaluation was computed (CudaHawkes.lastEvaluationPath).
+PATH_SWEEP = 0
+PATH_INCREMENTAL = 1
+PATH_KEPT_SUMS = 2
 
 PRECISION_FP64 = 0
 PRECISION_FP32_COMP = 1
@@ -241,6 +247,14 @@ class CudaHawkes:
         evaluated once for both of its events counts once)."""
         v = ctypes.c_double()
         self._check(_lib.hphc_get_last_launch_evals(self._h, ctypes.byref(v)), "lastLaunchEvals")
+        return v.value
+
+    @property
+    def lastEvaluationPath(self) -> int:
+        """PATH_SWEEP, PATH_INCREMENTAL or PATH_KEPT_SUMS for the last evaluation."""
+        v = ctypes.c_int()
+        self._check(_lib.hphc_get_last_evaluation_path(self._h, ctypes.byref(v)),
+                    "lastEvaluationPath")
         return v.value
 
 

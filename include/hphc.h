@@ -72,6 +72,15 @@ extern "C" {
 #define HPHC_FLAG_FP32_ORDERED (1L << 13)    /* evaluate both orders of every background
                                                 pair (by default each pair is evaluated
                                                 once and added to both events' sums) */
+#define HPHC_FLAG_NO_INCREMENTAL (1L << 14)  /* always run the full pair sweep (by default
+                                                an evaluation at unchanged parameters after
+                                                a few single-event updateLocations calls
+                                                updates the kept per-event sums in O(N)) */
+
+/* How the last evaluation was computed (hphc_get_last_evaluation_path). */
+#define HPHC_PATH_SWEEP 0        /* the O(N^2) pair sweep                             */
+#define HPHC_PATH_INCREMENTAL 1  /* kept sums updated for moved events, O(N) each     */
+#define HPHC_PATH_KEPT_SUMS 2    /* nothing changed since the sums were kept: O(N) finish */
 
 /* Precision modes reported by hphc_get_precision(). */
 #define HPHC_PRECISION_FP64 0          /* plain FP64 pair terms and reductions           */
@@ -146,7 +155,9 @@ int hphc_get_probs_self_excite(hphc_engine* engine, double* out, size_t length);
 /* Save parameters, locations and the last log-likelihood.  The reference's
  * NewHawkes::storeState copies in the wrong direction (src/NewHawkes.hpp:286-291);
  * this saves the current state, as OpenCLHawkes::storeState does
- * (src/backend/opencl/OpenCLHawkes.hpp:283-300). */
+ * (src/backend/opencl/OpenCLHawkes.hpp:283-300).  The kept per-event sums (if
+ * current) are saved too, so that an evaluation after restoreState needs no
+ * sweep. */
 int hphc_store_state(hphc_engine* engine);
 
 /* Return to the saved state (src/NewHawkes.hpp:305-318).  The saved
@@ -198,6 +209,53 @@ int hphc_multiset_get_last_launch_stats(hphc_multiset* multiset, int* kernelLaun
                                         double* backgroundTerms, double* selfExciteTerms);
 int hphc_multiset_get_last_launch_evals(hphc_multiset* multiset, double* backgroundEvals);
 
+/* ---- multi-chain Metropolis-Hastings sampler ----------------------------
+ *
+ * Replaces the reference's R sampler() (R/Untitled.R:254-422) and its
+ * Potential() (:225-231) for numChains independent chains whose proposals are
+ * evaluated together: one batched likelihood run per iteration.  Each chain
+ * follows the reference loop: random-scan choice of one sampled parameter, a
+ * proposal from a normal truncated to (0, inf) centred on the current value
+ * (sd = that parameter's radius), truncated-normal priors (sd 10 for the first
+ * five parameters, 1 for mu0), the Metropolis-Hastings test with the proposal
+ * densities, radius adaptation towards 0.44 acceptance every SampBound
+ * proposals (SampBound from 5, growing to ceil(SampBound^1.1)).  Random
+ * numbers come from one splitmix64 stream per chain seeded from `seed` and the
+ * chain index (the reference uses R's generator), so runs are reproducible.
+ *
+ * initialParams: numChains x 6.  radius: initial proposal sd of every
+ * parameter (the reference's `radius`, default 2).  sampledMask: bit q set =
+ * parameter q is proposed; 0 selects the reference's set {sigma, omega,
+ * theta, mu0} (sample(c(1,4:6)), R/Untitled.R:328).  The sampler keeps its
+ * state between runs. */
+typedef struct hphc_sampler hphc_sampler;
+
+/* Batched log-likelihood evaluator for hphc_sampler_run_with: K parameter
+ * vectors (K x 6) in, K log-likelihoods out; returns 0 on success. */
+typedef int (*hphc_batch_loglik_fn)(void* user, const double* params, int K, double* loglik);
+
+int hphc_sampler_create(int numChains, const double* initialParams, double radius,
+                        int sampledMask, unsigned long long seed, hphc_sampler** out);
+void hphc_sampler_destroy(hphc_sampler* sampler);
+const char* hphc_sampler_last_error(const hphc_sampler* sampler);
+
+/* Run `iterations` iterations of every chain on the engine's events (the
+ * engine's own parameters are not changed).  samples (numChains x
+ * (iterations - burnIn) x 6) and targets (numChains x (iterations - burnIn),
+ * the potential -logL - log prior, the reference's `target`) may be null. */
+int hphc_sampler_run(hphc_sampler* sampler, hphc_engine* engine, int iterations, int burnIn,
+                     double* samples, double* targets);
+
+/* The same with a caller-supplied batched evaluator. */
+int hphc_sampler_run_with(hphc_sampler* sampler, hphc_batch_loglik_fn evaluate, void* user,
+                          int iterations, int burnIn, double* samples, double* targets);
+
+/* Current state per chain (each pointer may be null): parameters (numChains x
+ * 6), potential (NaN before the first run), radii (numChains x 6), accepted
+ * and proposed counts. */
+int hphc_sampler_get_state(const hphc_sampler* sampler, double* params, double* potential,
+                           double* radii, long long* accepted, long long* proposed);
+
 /* ---- evaluation without allocation (no reference counterpart) -----------
  *
  * FP64 log-likelihood and gradient of one event set for callers that must not
@@ -242,6 +300,19 @@ int hphc_enqueue_log_likelihood_and_gradient(hphc_engine* engine);
 /* Wait for the last enqueued evaluation and copy its log-likelihood and
  * gradient (6, may be null) to the host. */
 int hphc_read_results(hphc_engine* engine, double* loglik, double* gradient, size_t length);
+
+/* Which path the most recent single evaluation took (HPHC_PATH_*).
+ * Incremental evaluation (no reference counterpart; the reference recomputes
+ * the O(N^2) sum on every call): after an evaluation the engine keeps each
+ * event's six unit pair sums.  If only a few events then move
+ * (hphc_update_locations with an index; at most max(1, min(64, N/512)) since
+ * the sums were formed) and the parameters are the same, the next evaluation
+ * updates every event's sums by its pair with each moved event and recomputes
+ * the moved events' own rows, O(N) per moved event, then re-runs the O(N)
+ * finish.  Changing the times, all locations (index -1) or moving more events
+ * falls back to the sweep.  Results agree with the sweep to FP64 rounding of
+ * the updates (FP64 mode) or to the FP32 mode's own accuracy. */
+int hphc_get_last_evaluation_path(hphc_engine* engine, int* path);
 
 /* Kernel launches made by the most recent evaluation call (for launch
  * accounting), and how many background and self-excitation pair terms its
