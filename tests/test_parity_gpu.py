@@ -152,9 +152,10 @@ def test_underflow_skip_is_bit_exact(flags):
         b.setSweepShape(2, 16)
         la, ga = a.getLogLikelihoodAndGradient()
         lb, gb = b.getLogLikelihoodAndGradient()
-        pa, pb = a.getProbsSelfExcite(), b.getProbsSelfExcite()
+        # stats of the sweeps (the probabilities below come from the kept sums)
         _, nba, nsa = a.lastLaunchStats()
         _, nbb, nsb = b.lastLaunchStats()
+        pa, pb = a.getProbsSelfExcite(), b.getProbsSelfExcite()
     assert la == lb and np.array_equal(ga, gb) and np.array_equal(pa, pb)
     assert nba + nsa < nbb + nsb  # the skip did remove work
     assert nbb == 20000.0 ** 2  # without it every background term is evaluated
