@@ -238,6 +238,54 @@ def cpu_baseline(budget_s=15.0):
 
 # ------------------------------------------------------------------ our arm --
 
+class Ranks:
+    """One process per GPU: the process group, barriers and the max-over-ranks
+    reduction of device times.  backend "nccl" on GPUs (the bench), "gloo" on
+    CPU (the multi-process tests); world 1 needs no process group."""
+
+    def __init__(self, world: int, backend: str = "nccl", device=None, timeout_s: int = 120):
+        import torch
+        self.world = world
+        self.device = device
+        self.dist = None
+        if world > 1:
+            import datetime
+
+            import torch.distributed as dist
+            kw = {"device_id": device} if backend == "nccl" else {}
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s), **kw)
+            self.dist = dist
+        self._torch = torch
+
+    def barrier(self):
+        cuda = self.device is not None and self.device.type == "cuda"
+        if cuda:
+            self._torch.cuda.synchronize()
+        if self.dist:
+            self.dist.barrier()
+        if cuda:
+            self._torch.cuda.synchronize()
+
+    def max(self, values):
+        """Elementwise maximum over ranks of a list of floats (every rank calls it)."""
+        t = self._torch.tensor([float(v) for v in values], dtype=self._torch.float64,
+                               device=self.device)
+        if self.dist:
+            self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return [float(v) for v in t.cpu()]
+
+    def close(self):
+        if self.dist:
+            self.dist.barrier()
+            self.dist.destroy_process_group()
+            self.dist = None
+
+
+def whole_job_rate(world: int, units_per_rank: float, ms_max: float) -> float:
+    """Units all ranks processed per second, over the slowest rank's time."""
+    return world * units_per_rank / (ms_max / 1e3)
+
+
 class Runner:
     """One workload on one GPU: the timed step through the engine (data on the
     device, CUDA-event step time recorded by the engine on its stream) and the
@@ -368,22 +416,11 @@ def ours_arm(args):
 
     rank, world, local = env_int("RANK", 0), env_int("WORLD_SIZE", 1), env_int("LOCAL_RANK", 0)
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+    ranks = Ranks(world, "nccl", torch.device("cuda", local))
+    barrier = ranks.barrier
 
     w = make_workload(args.workload, args.n)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{local}")
-
-    def barrier():
-        torch.cuda.synchronize()
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize()
 
     def flusher(run):
         if run.stream:
@@ -399,6 +436,9 @@ def ours_arm(args):
 
     fp32 = Runner(hb, w, hb.CUDA | hb.COMPENSATED, local)
     fp64 = Runner(hb, w, hb.CUDA, local)
+    if args.shape and w["kind"] != "sets":
+        r_, i_ = (int(v) for v in args.shape.split(":"))
+        fp32.eng.setSweepShape(r_, i_)
 
     # FP64 plain path (the comparison in the metric)
     barrier()
@@ -416,32 +456,23 @@ def ours_arm(args):
     _, nb64, ns64 = fp64.eng.lastLaunchStats()
     steps64 = args.steps64 or args.steps
 
-    tot = torch.tensor([sum(ms32) / args.steps, sum(ms64) / steps64], dtype=torch.float64,
-                       device=f"cuda:{local}")
-    if dist:
-        dist.all_reduce(tot, op=dist.ReduceOp.MAX)
-    ms_step32, ms_step64 = float(tot[0]), float(tot[1])
+    ms_step32, ms_step64 = ranks.max([sum(ms32) / args.steps, sum(ms64) / steps64])
 
     # End to end through the public API with host buffers.
     fp64.close()
     barrier()
     e2e_s = time_e2e(fp32, max(1, min(args.steps, 50)), args.warmup)
-    e2e_t = torch.tensor([e2e_s], dtype=torch.float64, device=f"cuda:{local}")
-    if dist:
-        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-    e2e_s = float(e2e_t[0])
+    e2e_s = ranks.max([e2e_s])[0]
 
     clock_summary = clocks.summary(None)
     fp32.close()
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    ranks.close()
     if rank != 0:
         return 0
 
     pairs = w["pairs"]
-    value = world * pairs / (ms_step32 / 1e3)
-    value64 = world * pairs / (ms_step64 / 1e3)
+    value = whole_job_rate(world, pairs, ms_step32)
+    value64 = whole_job_rate(world, pairs, ms_step64)
     peaks, peak_src = measured_peaks()
     sm_count = torch.cuda.get_device_properties(local).multi_processor_count
     max_mhz = float(peaks.get("sm_max_mhz", 1965.0))
@@ -509,7 +540,7 @@ def ours_arm(args):
                                             "the earlier event's sums + 5 per self-excitation "
                                             "term"},
                      "sweep_ms": sweep_mean},
-        "e2e": {"value": world * pairs / e2e_s, "unit": UNIT,
+        "e2e": {"value": whole_job_rate(world, pairs, 1e3 * e2e_s), "unit": UNIT,
                 "h2d_bytes_per_step": w["h2d"], "d2h_bytes_per_step": w["d2h"]},
         "gpu_launches": launches * args.steps,
         "clocks": clock_summary,
@@ -534,6 +565,9 @@ def main():
     ap.add_argument("--steps64", type=int, default=0,
                     help="timed steps of the FP64 comparison (default: --steps)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--shape", default="",
+                    help="fix the sweep shape as R:ITEMS_PER_SM instead of autotuning it "
+                         "(e.g. to profile one shape)")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)

@@ -4,7 +4,7 @@ The compute path is libhawkes_b200.so (hand-written sm_100a CUDA kernels behind
 the C ABI in include/hphc.h); this package is its Python host interface.
 """
 from .engine import (  # noqa: F401
-    AVX, AVX512, COMPENSATED, CUDA, FLOAT, FP32_FAST_EXP, FP32_ORDERED, FP32_SPACE_HILO,
+    AVX, AVX512, COMPENSATED, CUDA, FLOAT, FP32_FAST_EXP, FP32_ORDERED, FP32_SPACE_HILO, ORDERED,
     NO_INCREMENTAL, NO_UNDERFLOW_SKIP,
     OPENCL, PARAMETER_NAMES, PATH_INCREMENTAL, PATH_KEPT_SUMS, PATH_SWEEP,
     PRECISION_FP32_COMP, PRECISION_FP64, SSE, TBB, CudaHawkes, Engine, HawkesError, Multiset,

@@ -72,14 +72,14 @@ int Executor::cuda_fail(cudaError_t e, const char* what) {
 }
 
 int Executor::init(int D, int precision, int variant, bool underflowSkip, int device,
-                   cudaStream_t stream, float ex2Fix) {
+                   cudaStream_t stream, double ex2Bias) {
     D_ = D;
     precision_ = precision;
     variant_ = variant;
     skip_ = underflowSkip;
     device_ = device;
     stream_ = stream;
-    ex2Fix_ = ex2Fix;
+    ex2Bias_ = ex2Bias;
     cudaDeviceGetAttribute(&numSMs_, cudaDevAttrMultiProcessorCount, device);
     R = precision == HPHC_PRECISION_FP64 ? 2 : 4;
     itemsPerSM = 32;
@@ -130,7 +130,6 @@ PairConsts Executor::pair_consts(const double* p) const {
         split_float(-(sigma * sigma) / (a * a), c.fSh, c.fSl);
         split_float(-omega * kLog2e / sT, c.fWh, c.fWl);
     }
-    c.ex2Fix = (precision_ == HPHC_PRECISION_FP64 || (variant_ & 2)) ? 0.0f : ex2Fix_;
     const double thr = precision_ == HPHC_PRECISION_FP64 ? kSkipF64 : kSkipF32;
     c.skipB = (skip_ && c.cB < 0.0 && c.cA <= 0.0) ? thr : -1.0;
     c.skipS = (skip_ && c.cW < 0.0 && c.cS <= 0.0) ? thr : -1.0;
@@ -155,6 +154,8 @@ FinishConsts Executor::finish_consts(const double* p, const SetView& set) const 
         f.accScale[1] = f.accScale[4] = 1.0 / (sX * sX);  // sums of d'^2
         f.accScale[2] = 1.0 / (sT * sT);                  // sum of dt'^2
         f.accScale[5] = 1.0 / sT;                         // sum of dt'
+        if (!(variant_ & 2))  // hardware exponential: divide out its mean relative error
+            for (int q = 0; q < kNumAcc; ++q) f.accScale[q] /= 1.0 + ex2Bias_;
     }
     f.T = set.hTimes[set.N - 1];
     // src/NewHawkes.hpp:659: locationCount * (embeddingDimension - 1) * log(M_1_SQRT_2PI)
@@ -224,11 +225,28 @@ int Executor::build_plan(const std::vector<SetView>& sets, const int* setOf, con
         sp.tileMax = s.dTileMax;
         sp.partials = reinterpret_cast<double*>(partOff);  // offset, fixed up later
         partOff += (size_t)maxChunks * kNumAcc * Npad;
-        sp.symmetric = (fp32 && symmetric && N <= kMaxSymmetricEvents) ? 1 : 0;
+        sp.symmetric = (symmetric && N <= kMaxSymmetricEvents) ? 1 : 0;
+        if (!fp32 && sp.symmetric) {
+            // FP64 column sums are fixed point: bound each column total by N
+            // times the largest term, B_u <= 1, B_u d^2 <= 1/(e |cA|),
+            // B_u dt^2 <= 1/(e |cB|), and keep it below 2^62 units.  Padding
+            // rows 1e150 away vanish only if |cA| is not astronomically small.
+            if (!(sp.c.cA < -1e-280 && sp.c.cB < 0.0)) {
+                sp.symmetric = 0;
+            } else {
+                const double e1 = std::exp(1.0);
+                const double bound[3] = {(double)N, N / (e1 * -sp.c.cA), N / (e1 * -sp.c.cB)};
+                for (int q = 0; q < 3; ++q) {
+                    int ex = 0;
+                    std::frexp(bound[q], &ex);  // bound < 2^ex
+                    sp.colShift[q] = 62 - ex;
+                }
+            }
+        }
         sp.colAcc = nullptr;
         if (sp.symmetric) {
             sp.colAcc = reinterpret_cast<unsigned long long*>(colOff + 1);  // offset + 1
-            colOff += (size_t)3 * Npad;
+            colOff += (size_t)(fp32 ? 3 : 6) * Npad;
         }
         if (fp32) {
             sp.rec = reinterpret_cast<const void*>(recOff);  // offset, fixed up later
@@ -313,6 +331,8 @@ int Executor::build_plan(const std::vector<SetView>& sets, const int* setOf, con
         fp.stripEvents = stripEvents;
         fp.blockBase = blockBase;
         fp.nBlocks = finish_blocks(N);
+        fp.colWords = fp32 ? 1 : 2;
+        for (int q = 0; q < 4; ++q) fp.colShift[q] = sp.colShift[q];
         fp.f = finish_consts(prm, s);
         for (int b = 0; b < fp.nBlocks; ++b) pl.fb.push_back(FinishBlock{p, b * kFinishThreads});
         blockBase += fp.nBlocks;

@@ -50,9 +50,10 @@ struct RunStats {
 class Executor {
 public:
     // precision: HPHC_PRECISION_*; variant: FP32 variant bits (see
-    // hphc_kernels.cu); ex2Fix: exponent offset for the hardware exponential.
+    // hphc_kernels.cu); ex2Bias: mean relative error of the hardware
+    // exponential (divided out of the sums when the variant uses it).
     int init(int D, int precision, int variant, bool underflowSkip, int device, cudaStream_t stream,
-             float ex2Fix);
+             double ex2Bias);
     void release();
 
     // Plan and enqueue P problems (problem p = set setOf[p] at params[6p..6p+5])
@@ -74,7 +75,7 @@ public:
     int R = 2, itemsPerSM = 16;      // shape in use
     bool useGraph = true;
     bool kernelTiming = false;
-    bool symmetric = false;  // FP32: symmetric background sweep (set before the first enqueue)
+    bool symmetric = false;  // symmetric background sweep (set before the first enqueue)
     double* sumsOut = nullptr;  // if set, problem 0's unit pair sums ([6][N], natural units)
     float lastSweepMs = 0.f, lastFinishMs = 0.f, lastStepMs = 0.f;
     bool timedValid = false;
@@ -83,7 +84,7 @@ public:
 private:
     int D_ = 0, precision_ = 0, variant_ = 0, device_ = 0, numSMs_ = 148;
     bool skip_ = true;
-    float ex2Fix_ = 0.f;
+    double ex2Bias_ = 0.0;
     cudaStream_t stream_ = nullptr;
     bool tuned_ = false;
 

@@ -16,6 +16,7 @@
 // All sums are written per (chunk, event) and combined in chunk order, then
 // reduced over events with fixed shuffle trees: results do not depend on
 // scheduling.
+#include <limits.h>
 #include <math.h>
 
 #include "hphc_kernels.cuh"
@@ -192,25 +193,141 @@ __device__ __forceinline__ void body_f64(const double* __restrict__ sRec, int nj
     }
 }
 
+// ---- symmetric FP64 background tiles ----
+//
+// As in the FP32 sweep, a tile before the strip evaluates each background
+// pair once and adds its three weighted terms to the row (registers) and to
+// the column.  Column partials are reduced per warp in groups of 4 columns:
+// lane l visits the group's columns in the order m ^ p, p = (l >> 3) & 3, so
+// after the loop cp[.][m] holds column m ^ p over the lane's R rows; shuffles
+// at distances 16 and 8 each keep the half of the columns the lane ends with,
+// then 4, 2 and 1 sum, leaving lanes 8p .. 8p + 7 with the warp total of
+// column p.  The 4 warp totals are added in FP64 in warp order and added to
+// the column's two-word fixed-point sum (see add_fixed2), so the result does
+// not depend on CTA order and keeps FP64 accuracy.
+
+constexpr int kSymGroup64 = 4;  // columns per warp exchange (FP64)
+
+// Adds v >= 0 to a two-word fixed-point sum: hi counts units of 2^-shift,
+// lo units of 2^-(shift + kColLoBits).  The host chooses shift so that no
+// column total exceeds 2^62 units; the lo word takes at most 2^23 additions
+// of values below 2^kColLoBits without overflowing.
+__device__ __forceinline__ void add_fixed2(unsigned long long* hi, unsigned long long* lo,
+                                           double v, int shift) {
+    const double scaled = ldexp(v, shift);
+    const double whole = floor(scaled);
+    atomicAdd(hi, (unsigned long long)whole);
+    atomicAdd(lo, (unsigned long long)rint(ldexp(scaled - whole, kColLoBits)));
+}
+
+template <int D, int R, bool DO_S, bool MASK>
+__device__ __forceinline__ void tile_sym_f64(const double* __restrict__ sRec,
+                                             const double (&xi)[R][D], const double (&ti)[R],
+                                             const PairConsts& c, double (&acc)[R][kNumAcc],
+                                             double* __restrict__ sCol,
+                                             unsigned long long* __restrict__ colAcc, int Npad,
+                                             int j0, const int (&shift)[3]) {
+    static_assert(kSweepThreads == kTile, "one column per thread in the column flush");
+    constexpr int S = Layout<D>::kF64Stride;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int p = (lane >> 3) & 3;
+#pragma unroll 1
+    for (int g = 0; g < kTile; g += kSymGroup64) {
+        double cp[3][kSymGroup64];
+#pragma unroll
+        for (int m = 0; m < kSymGroup64; ++m) {
+            const int j = g + (m ^ p);
+            double rj[S];
+#pragma unroll
+            for (int v = 0; v < S / 2; ++v) {
+                const double2 q = reinterpret_cast<const double2*>(sRec + j * S)[v];
+                rj[2 * v] = q.x;
+                rj[2 * v + 1] = q.y;
+            }
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                double d2 = 0.0;
+#pragma unroll
+                for (int k = 0; k < D; ++k) {
+                    const double dd = xi[r][k] - rj[k];
+                    d2 = fma(dd, dd, d2);
+                }
+                const double dt = ti[r] - rj[D];
+                const double t2 = dt * dt;
+                const double B = exp(fma(c.cA, d2, c.cB * t2));
+                const double Bd = B * d2, Bt = B * t2;
+                acc[r][0] += B;
+                acc[r][1] += Bd;
+                acc[r][2] += Bt;
+                if (r == 0) {
+                    cp[0][m] = B;
+                    cp[1][m] = Bd;
+                    cp[2][m] = Bt;
+                } else {
+                    cp[0][m] += B;
+                    cp[1][m] += Bd;
+                    cp[2][m] += Bt;
+                }
+                if (DO_S) {
+                    double Sv = exp(fma(c.cS, d2, c.cW * dt));
+                    if (MASK) Sv = dt > 0.0 ? Sv : 0.0;
+                    acc[r][3] += Sv;
+                    acc[r][4] = fma(Sv, d2, acc[r][4]);
+                    acc[r][5] = fma(Sv, dt, acc[r][5]);
+                }
+            }
+        }
+        constexpr unsigned kAll = 0xffffffffu;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            const double u0 = cp[q][0] + __shfl_xor_sync(kAll, cp[q][2], 16);
+            const double u1 = cp[q][1] + __shfl_xor_sync(kAll, cp[q][3], 16);
+            double w = u0 + __shfl_xor_sync(kAll, u1, 8);
+            w += __shfl_xor_sync(kAll, w, 4);
+            w += __shfl_xor_sync(kAll, w, 2);
+            w += __shfl_xor_sync(kAll, w, 1);
+            if ((lane & 7) == 0) sCol[(warp * 3 + q) * kTile + g + p] = w;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        double v = 0.0;
+#pragma unroll
+        for (int w = 0; w < kSweepThreads / 32; ++w) v += sCol[(w * 3 + q) * kTile + tid];
+        add_fixed2(colAcc + (size_t)(2 * q) * Npad + j0 + tid,
+                   colAcc + (size_t)(2 * q + 1) * Npad + j0 + tid, v, shift[q]);
+    }
+}
+
 // One work item of the FP64 sweep: target strip `strip` (kSweepThreads * R
 // events) against j tiles [jt0, jt1); unit pair sums to partial slot `slot`.
+// sym: tiles before the strip are evaluated once per pair (rows + columns).
 template <int D, int R>
 __device__ __forceinline__ void f64_item(const double* __restrict__ rec,
                                          const double* __restrict__ tileMin,
                                          const double* __restrict__ tileMax,
                                          double* __restrict__ partials, int N, int nTiles,
                                          int Npad, const PairConsts& c, int strip, int jt0,
-                                         int jt1, int slot, double* sRec) {
+                                         int jt1, int slot, double* sRec, bool sym,
+                                         unsigned long long* __restrict__ colAcc,
+                                         const int (&shift)[3], double* sCol) {
     constexpr int S = Layout<D>::kF64Stride;
     const int tid = threadIdx.x;
     const int stripBase = strip * kSweepThreads * R;
+    const int ts0 = stripBase / kTile, ts1 = min(ts0 + R, nTiles);
 
     double xi[R][D], ti[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-        const int i = min(stripBase + r * kSweepThreads + tid, N - 1);
+        const int iRaw = stripBase + r * kSweepThreads + tid;
+        const int i = min(iRaw, N - 1);
 #pragma unroll
-        for (int k = 0; k < D; ++k) xi[r][k] = rec[(size_t)i * S + k];
+        for (int k = 0; k < D; ++k)
+            // padding rows of the last strip sit 1e150 away: every background
+            // term they form is exactly 0, so they add nothing to column sums
+            xi[r][k] = iRaw < N ? rec[(size_t)i * S + k] : 1e150;
         ti[r] = rec[(size_t)i * S + D];
     }
     double tminI = INFINITY, tmaxI = -INFINITY;
@@ -229,7 +346,8 @@ __device__ __forceinline__ void f64_item(const double* __restrict__ rec,
         for (int q = 0; q < kNumAcc; ++q) acc[r][q] = 0.0;
 
     for (int jt = jt0; jt < jt1; ++jt) {
-        const TileMode m = tile_mode(tminI, tmaxI, tileMin[jt], tileMax[jt], c);
+        TileMode m = tile_mode(tminI, tmaxI, tileMin[jt], tileMax[jt], c);
+        if (sym && jt >= ts1) m.doB = false;  // covered as columns by later strips
         if (!m.doB && !m.doS) continue;
         const int j0 = jt * kTile;
         const int nj = min(kTile, N - j0);
@@ -238,7 +356,18 @@ __device__ __forceinline__ void f64_item(const double* __restrict__ rec,
         double2* dst = reinterpret_cast<double2*>(sRec);
         for (int v = tid; v < nj * (S / 2); v += kSweepThreads) dst[v] = src[v];
         __syncthreads();
-        if (m.doB) {
+        if (sym && m.doB && jt < ts0) {
+            // jt < ts0 <= nTiles - 1: a full tile
+            if (!m.doS)
+                tile_sym_f64<D, R, false, false>(sRec, xi, ti, c, acc, sCol, colAcc, Npad, j0,
+                                                 shift);
+            else if (m.allCausal)
+                tile_sym_f64<D, R, true, false>(sRec, xi, ti, c, acc, sCol, colAcc, Npad, j0,
+                                                shift);
+            else
+                tile_sym_f64<D, R, true, true>(sRec, xi, ti, c, acc, sCol, colAcc, Npad, j0,
+                                               shift);
+        } else if (m.doB) {
             if (!m.doS)
                 body_f64<D, R, true, false, false>(sRec, nj, xi, ti, c, acc);
             else if (m.allCausal)
@@ -274,8 +403,9 @@ sweep_f64_kernel(SweepGeometry g, const double* __restrict__ rec,
     const int chunk = blockIdx.x - strip * g.nChunks;
     const int jt0 = chunk * g.chunkTiles;
     const int jt1 = min(jt0 + g.chunkTiles, g.nTiles);
+    const int noShift[3] = {0, 0, 0};
     f64_item<D, R>(rec, tileMin, tileMax, partials, g.N, g.nTiles, g.Npad, c, strip, jt0, jt1,
-                   chunk, sRec);
+                   chunk, sRec, false, nullptr, noShift, nullptr);
 }
 
 // Takes the next work-list index for the CTA (all threads get the same one).
@@ -293,6 +423,7 @@ sweep_f64_list_kernel(const SweepProblem* __restrict__ problems,
                       const WorkItem* __restrict__ items, const int* __restrict__ nItems,
                       int* __restrict__ counter) {
     __shared__ __align__(16) double sRec[kTile * Layout<D>::kF64Stride];
+    __shared__ __align__(16) double sCol[(kSweepThreads / 32) * 3 * kTile];
     __shared__ int sNext;
     const int n = *nItems;
     for (;;) {
@@ -301,8 +432,10 @@ sweep_f64_list_kernel(const SweepProblem* __restrict__ problems,
         const WorkItem w = items[it];
         const SweepProblem& P = problems[w.problem];
         const PairConsts c = P.c;
+        const int shift[3] = {P.colShift[0], P.colShift[1], P.colShift[2]};
         f64_item<D, R>(static_cast<const double*>(P.rec), P.tileMin, P.tileMax, P.partials, P.N,
-                       P.nTiles, P.Npad, c, w.strip, w.jt0, w.jt1, w.slot, sRec);
+                       P.nTiles, P.Npad, c, w.strip, w.jt0, w.jt1, w.slot, sRec,
+                       P.symmetric != 0, P.colAcc, shift, sCol);
     }
 }
 
@@ -326,8 +459,9 @@ sweep_f64_list_kernel(const SweepProblem* __restrict__ problems,
 //   kSpaceLo  coordinate differences use the lo parts too (else hi only: the
 //             coordinate rounding then acts as a fixed ~1e-7 relative
 //             perturbation of each event's location, unbiased across events).
-//   kPolyExp  exponentials by exp2_poly (unbiased to ~3e-10) instead of
-//             ex2.approx with the measured mean-bias offset.
+//   kPolyExp  exponentials by exp2_poly_neg2 (unbiased to ~3e-10) instead of
+//             ex2.approx, whose measured mean relative error the finish
+//             divides out of the sums.
 constexpr int kSpaceLo = 1;
 constexpr int kPolyExp = 2;
 
@@ -342,103 +476,162 @@ constexpr float kP5 = 0x1.5da248p-10f;
 constexpr float kP6 = 0x1.43ec02p-13f;
 constexpr float kP7 = 0x1.e50106p-17f;
 
-// 2^x by Cody-Waite reduction x = n + f, n = rint(x), |f| <= 1/2 (f exact),
-// p(f) by Horner on the FMA pipe, and the scale 2^n from ex2.approx.ftz on the
-// integer n: that instruction returns exactly 2^n for every integer n (checked
-// on the device for n in [-200, 130]), +0 for n <= -127 and +inf above 127, so
-// the scale needs no clamp or exponent-field arithmetic and any |x| is safe
-// (for |x| >= 2^23, f = 0).  Arguments below -126.5 give +0 as with
-// ex2.approx.ftz, so the tile-level underflow skip stays exact.  The hardware
-// approximation error never enters: only the exact power of two is taken from
-// it, the fractional part is the polynomial's.
-__device__ __forceinline__ float exp2_poly(float x) {
-    const float n = rintf(x);
-    const float f = x - n;
-    float p = kP7;
-    p = fmaf(p, f, kP6);
-    p = fmaf(p, f, kP5);
-    p = fmaf(p, f, kP4);
-    p = fmaf(p, f, kP3);
-    p = fmaf(p, f, kP2);
-    p = fmaf(p, f, kP1);
-    p = fmaf(p, f, 1.0f);
-    return p * ex2_ftz(n);
+// ---- packed column pairs ----
+//
+// sm_100 executes FP32 add, multiply and fused multiply-add on float2
+// operands (one instruction, two results).  The sweep is bound by
+// instruction issue, so each thread evaluates two consecutive columns
+// (j, j+1) of a target row in one float2 throughout: differences, exponents,
+// the exponential's polynomial and the weighted sums.  The staged tile is a
+// structure of arrays (one array per record field, column values negated so
+// that differences are additions), so one 8-byte shared load yields a field
+// of a column pair; row values are held duplicated in both halves.  A tile
+// with an odd number of events is padded with one column whose coordinate
+// and time are 1e18 away, so all its terms are exactly zero.
+
+__device__ __forceinline__ float2 dup2(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
+// 2^(-s) for both halves by Cody-Waite reduction: m = rint(s), f = m - s in
+// [-1/2, 1/2] (exact), p(f) by packed Horner on the FMA pipe, times the exact
+// power 2^-m from ex2.approx.ftz on the integer -m.  That instruction returns
+// exactly 2^n for every integer n (checked on the device for n in [-200,
+// 130]), +0 for n <= -127 and +inf above 127, so the scale needs no clamp or
+// exponent-field arithmetic and any |s| is safe (for |s| >= 2^23, f = 0).
+// Arguments s above 126.5 give +0 as with ex2.approx.ftz, so the tile-level
+// underflow skip stays exact.  The hardware approximation error never
+// enters: only the exact power of two is taken from it, the fractional part
+// is the polynomial's.
+__device__ __forceinline__ float2 exp2_poly_neg2(float2 s) {
+    const float2 m = make_float2(rintf(s.x), rintf(s.y));
+    const float2 f = fma2(s, dup2(-1.0f), m);
+    float2 p = fma2(dup2(kP7), f, dup2(kP6));
+    p = fma2(p, f, dup2(kP5));
+    p = fma2(p, f, dup2(kP4));
+    p = fma2(p, f, dup2(kP3));
+    p = fma2(p, f, dup2(kP2));
+    p = fma2(p, f, dup2(kP1));
+    p = fma2(p, f, dup2(1.0f));
+    return mul2(p, make_float2(ex2_ftz(-m.x), ex2_ftz(-m.y)));
 }
 
+// Background unit terms 2^-(d2 + t2).  The hardware exponential's mean
+// relative error is divided out of the sums in the FP64 finish.
 template <int V>
-__device__ __forceinline__ float exp2_term(float e) {
-    if (V & kPolyExp) return exp2_poly(e);
-    return ex2_ftz(e);
+__device__ __forceinline__ float2 background2(float2 s) {
+    if (V & kPolyExp) return exp2_poly_neg2(s);
+    return make_float2(ex2_ftz(-s.x), ex2_ftz(-s.y));
 }
 
-template <int D, int R, int V, bool DO_B, bool DO_S, bool MASK>
-__device__ __forceinline__ void body_f32(const float* __restrict__ sRec, int jb, int je,
-                                         const float (&xh)[R][D], const float (&xl)[R][D],
-                                         const float (&th)[R], const float (&tl)[R],
-                                         const int (&rk)[R], const PairConsts& c,
-                                         float (&a)[R][kNumAcc]) {
-    constexpr int S = Layout<D>::kF32Stride;
-#pragma unroll 4
-    for (int j = jb; j < je; ++j) {
-        float rj[S];
+// Unit self-excitation terms of a column pair, zeroed where t_j >= t_i when
+// MASK (ranks: equal times share one).
+template <int V, bool MASK>
+__device__ __forceinline__ float2 self_excite2(float2 d2, float2 dt, int rank, int2 rj,
+                                               const PairConsts& c) {
+    const float2 e = fma2(dup2(c.fSh), d2,
+                          fma2(dup2(c.fWh), dt, fma2(dup2(c.fSl), d2, mul2(dup2(c.fWl), dt))));
+    const float ex = fminf(e.x, 127.0f), ey = fminf(e.y, 127.0f);
+    float2 S;
+    if (V & kPolyExp) S = exp2_poly_neg2(make_float2(-ex, -ey));
+    else S = make_float2(ex2_ftz(ex), ex2_ftz(ey));
+    if (MASK) {
+        S.x = rank > rj.x ? S.x : 0.0f;
+        S.y = rank > rj.y ? S.y : 0.0f;
+    }
+    return S;
+}
+
+// A staged tile: per field, kTile columns (+1 padding column), negated.
+template <int D>
+struct StagedTile {
+    static constexpr int kCols = kTile + 2;  // even stride, room for the padding column
+    float nx[D][kCols];   // -x'hi
+    float nxl[D][kCols];  // -x'lo
+    float nt[kCols];      // -t'hi
+    float ntl[kCols];     // -t'lo
+    int rank[kCols];
+};
+
+// Row values held duplicated for the packed arithmetic.
+template <int D, int R>
+struct Rows2 {
+    float2 xh[R][D], xl[R][D], th[R], tl[R];
+    int rk[R];
+};
+
+// Squared distance and time difference of row r against column pair p
+// (columns 2p, 2p+1 of the staged tile).
+template <int D, int R, int V>
+__device__ __forceinline__ void geometry2(const StagedTile<D>& t, int p, const Rows2<D, R>& w,
+                                          int r, float2& d2, float2& dt) {
 #pragma unroll
-        for (int v = 0; v < S / 4; ++v) {
-            const float4 q = reinterpret_cast<const float4*>(sRec + j * S)[v];
-            rj[4 * v] = q.x;
-            rj[4 * v + 1] = q.y;
-            rj[4 * v + 2] = q.z;
-            rj[4 * v + 3] = q.w;
-        }
+    for (int k = 0; k < D; ++k) {
+        float2 dd = add2(w.xh[r][k], reinterpret_cast<const float2*>(t.nx[k])[p]);
+        if (V & kSpaceLo) dd = add2(dd, add2(w.xl[r][k], reinterpret_cast<const float2*>(t.nxl[k])[p]));
+        d2 = k == 0 ? mul2(dd, dd) : fma2(dd, dd, d2);
+    }
+    dt = add2(add2(w.th[r], reinterpret_cast<const float2*>(t.nt)[p]),
+              add2(w.tl[r], reinterpret_cast<const float2*>(t.ntl)[p]));
+}
+
+// Row-order pass over column pairs [p0, p1) of the staged tile (broadcast
+// reads shared by the R rows).
+template <int D, int R, int V, bool DO_B, bool DO_S, bool MASK>
+__device__ __forceinline__ void body_f32(const StagedTile<D>& t, int p0, int p1,
+                                         const Rows2<D, R>& w, const PairConsts& c,
+                                         float2 (&a)[R][kNumAcc]) {
+#pragma unroll 2
+    for (int p = p0; p < p1; ++p) {
+        const int2 rj = MASK ? reinterpret_cast<const int2*>(t.rank)[p] : make_int2(0, 0);
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-            float d2 = 0.0f;
-#pragma unroll
-            for (int k = 0; k < D; ++k) {
-                const float dd = (V & kSpaceLo) ? (xh[r][k] - rj[k]) + (xl[r][k] - rj[D + 1 + k])
-                                                : xh[r][k] - rj[k];
-                d2 = fmaf(dd, dd, d2);
-            }
-            const float dt = (th[r] - rj[D]) + (tl[r] - rj[2 * D + 1]);
+            float2 d2, dt;
+            geometry2<D, R, V>(t, p, w, r, d2, dt);
             if (DO_B) {
-                const float t2 = dt * dt;
-                const float e = (V & kPolyExp) ? -(d2 + t2) : (c.ex2Fix - d2) - t2;
-                const float B = exp2_term<V>(e);
-                a[r][0] += B;
-                a[r][1] = fmaf(B, d2, a[r][1]);
-                a[r][2] = fmaf(B, t2, a[r][2]);
+                const float2 t2 = mul2(dt, dt);
+                const float2 B = background2<V>(add2(d2, t2));
+                a[r][0] = add2(a[r][0], B);
+                a[r][1] = fma2(B, d2, a[r][1]);
+                a[r][2] = fma2(B, t2, a[r][2]);
             }
             if (DO_S) {
-                const float e = fminf(
-                    fmaf(c.fSh, d2, fmaf(c.fWh, dt, fmaf(c.fSl, d2, fmaf(c.fWl, dt, c.ex2Fix)))),
-                    127.0f);
-                float Sv = exp2_term<V>(e);
-                if (MASK) Sv = rk[r] > __float_as_int(rj[2 * D + 2]) ? Sv : 0.0f;
-                a[r][3] += Sv;
-                a[r][4] = fmaf(Sv, d2, a[r][4]);
-                a[r][5] = fmaf(Sv, dt, a[r][5]);
+                const float2 S = self_excite2<V, MASK>(d2, dt, w.rk[r], rj, c);
+                a[r][3] = add2(a[r][3], S);
+                a[r][4] = fma2(S, d2, a[r][4]);
+                a[r][5] = fma2(S, dt, a[r][5]);
             }
         }
     }
 }
 
+template <int R>
+__device__ __forceinline__ void zero_rows(float2 (&a)[R][kNumAcc]) {
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+        for (int q = 0; q < kNumAcc; ++q) a[r][q] = make_float2(0.0f, 0.0f);
+}
+
+template <int R>
+__device__ __forceinline__ void flush_rows(const float2 (&a)[R][kNumAcc],
+                                           double (&acc)[R][kNumAcc]) {
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+        for (int q = 0; q < kNumAcc; ++q) acc[r][q] += (double)(a[r][q].x + a[r][q].y);
+}
+
 template <int D, int R, int V, bool DO_B, bool DO_S, bool MASK>
-__device__ __forceinline__ void tile_f32(const float* __restrict__ sRec, int nj,
-                                         const float (&xh)[R][D], const float (&xl)[R][D],
-                                         const float (&th)[R], const float (&tl)[R],
-                                         const int (&rk)[R], const PairConsts& c,
-                                         double (&acc)[R][kNumAcc]) {
-    for (int jb = 0; jb < nj; jb += kFlush) {
-        float a[R][kNumAcc];
-#pragma unroll
-        for (int r = 0; r < R; ++r)
-#pragma unroll
-            for (int q = 0; q < kNumAcc; ++q) a[r][q] = 0.0f;
-        body_f32<D, R, V, DO_B, DO_S, MASK>(sRec, jb, min(jb + kFlush, nj), xh, xl, th, tl, rk, c,
-                                            a);
-#pragma unroll
-        for (int r = 0; r < R; ++r)
-#pragma unroll
-            for (int q = 0; q < kNumAcc; ++q) acc[r][q] += (double)a[r][q];
+__device__ __forceinline__ void tile_f32(const StagedTile<D>& t, int nj, const Rows2<D, R>& w,
+                                         const PairConsts& c, double (&acc)[R][kNumAcc]) {
+    const int nPairs = (nj + 1) / 2;
+    for (int p0 = 0; p0 < nPairs; p0 += kFlush / 2) {
+        float2 a[R][kNumAcc];
+        zero_rows<R>(a);
+        body_f32<D, R, V, DO_B, DO_S, MASK>(t, p0, min(p0 + kFlush / 2, nPairs), w, c, a);
+        flush_rows<R>(a, acc);
     }
 }
 
@@ -446,138 +639,115 @@ __device__ __forceinline__ void tile_f32(const float* __restrict__ sRec, int nj,
 //
 // For a tile J before the strip, each pair (i, j) is evaluated once and its
 // background terms B, B d'^2, B dt'^2 go to row i (registers, as above) and
-// to column j.  Column sums are formed per warp in groups of 8 columns: lane
-// l visits the group's columns in the order jj ^ (l >> 2), so that after the
-// loop register cp[jj] of lane l holds column (jj ^ (l >> 2)) summed over the
-// lane's R rows; a transposing exchange (shuffles at distances 16, 8, 4 that
-// each keep the half of the columns the lane ends with, then 2 and 1) leaves
-// lane l with the warp total of column l >> 2, with no selects.  The 4 warp
-// totals of a column are added in FP64 in warp order and added to the
-// column's fixed-point sum, so the result does not depend on CTA order.
+// to column j.  Column sums are formed per warp in groups of 8 columns (4
+// column pairs): lane l visits the group's pairs in the order m ^ q, q =
+// (l >> 3) & 3, so that after the loop its accumulator c[m] holds column pair
+// m ^ q summed over the lane's R rows.  A transposing exchange -- float2
+// shuffles at distances 16 and 8 that each keep the half of the pairs the
+// lane ends with, a split of the pair at distance 4, then sums at 2 and 1 --
+// leaves lane l with the warp total of column (l >> 2), with no selects in
+// the loop.  The 4 warp totals of a column are added in FP64 in warp order
+// and added to the column's fixed-point sum, so the result does not depend
+// on CTA order.
 
 constexpr int kSymGroup = 8;  // columns per warp exchange
 
-template <int D, int R, int V, bool DO_S, bool MASK>
-__device__ __forceinline__ void sym_group_f32(const float* __restrict__ sRec, int g, int perm,
-                                              const float (&xh)[R][D], const float (&xl)[R][D],
-                                              const float (&th)[R], const float (&tl)[R],
-                                              const int (&rk)[R], const PairConsts& c,
-                                              float (&a)[R][kNumAcc],
-                                              float (&cp)[kSymGroup][3]) {
-    constexpr int S = Layout<D>::kF32Stride;
-#pragma unroll
-    for (int jj = 0; jj < kSymGroup; ++jj) {
-        const int j = g + (jj ^ perm);
-        float rj[S];
-#pragma unroll
-        for (int v = 0; v < S / 4; ++v) {
-            const float4 q = reinterpret_cast<const float4*>(sRec + j * S)[v];
-            rj[4 * v] = q.x;
-            rj[4 * v + 1] = q.y;
-            rj[4 * v + 2] = q.z;
-            rj[4 * v + 3] = q.w;
-        }
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            float d2 = 0.0f;
-#pragma unroll
-            for (int k = 0; k < D; ++k) {
-                const float dd = (V & kSpaceLo) ? (xh[r][k] - rj[k]) + (xl[r][k] - rj[D + 1 + k])
-                                                : xh[r][k] - rj[k];
-                d2 = fmaf(dd, dd, d2);
-            }
-            const float dt = (th[r] - rj[D]) + (tl[r] - rj[2 * D + 1]);
-            const float t2 = dt * dt;
-            const float e = (V & kPolyExp) ? -(d2 + t2) : (c.ex2Fix - d2) - t2;
-            const float B = exp2_term<V>(e);
-            a[r][0] += B;
-            a[r][1] = fmaf(B, d2, a[r][1]);
-            a[r][2] = fmaf(B, t2, a[r][2]);
-            if (r == 0) {
-                cp[jj][0] = B;
-                cp[jj][1] = B * d2;
-                cp[jj][2] = B * t2;
-            } else {
-                cp[jj][0] += B;
-                cp[jj][1] = fmaf(B, d2, cp[jj][1]);
-                cp[jj][2] = fmaf(B, t2, cp[jj][2]);
-            }
-            if (DO_S) {
-                const float es = fminf(
-                    fmaf(c.fSh, d2, fmaf(c.fWh, dt, fmaf(c.fSl, d2, fmaf(c.fWl, dt, c.ex2Fix)))),
-                    127.0f);
-                float Sv = exp2_term<V>(es);
-                if (MASK) Sv = rk[r] > __float_as_int(rj[2 * D + 2]) ? Sv : 0.0f;
-                a[r][3] += Sv;
-                a[r][4] = fmaf(Sv, d2, a[r][4]);
-                a[r][5] = fmaf(Sv, dt, a[r][5]);
-            }
-        }
-    }
+__device__ __forceinline__ float2 shfl_xor2(float2 v, int d) {
+    constexpr unsigned kAll = 0xffffffffu;
+    return make_float2(__shfl_xor_sync(kAll, v.x, d), __shfl_xor_sync(kAll, v.y, d));
 }
 
-// Warp total of column (lane >> 2) of the group from the permuted partials.
-__device__ __forceinline__ float sym_exchange(const float (&cp)[kSymGroup][3], int q) {
+// Warp total of column (lane >> 2) of the group.
+__device__ __forceinline__ float sym_exchange(const float2 (&cp)[kSymGroup / 2], bool hi) {
     constexpr unsigned kAll = 0xffffffffu;
-    const float u0 = cp[0][q] + __shfl_xor_sync(kAll, cp[4][q], 16);
-    const float u1 = cp[1][q] + __shfl_xor_sync(kAll, cp[5][q], 16);
-    const float u2 = cp[2][q] + __shfl_xor_sync(kAll, cp[6][q], 16);
-    const float u3 = cp[3][q] + __shfl_xor_sync(kAll, cp[7][q], 16);
-    const float w0 = u0 + __shfl_xor_sync(kAll, u2, 8);
-    const float w1 = u1 + __shfl_xor_sync(kAll, u3, 8);
-    float x = w0 + __shfl_xor_sync(kAll, w1, 4);
+    const float2 u0 = add2(cp[0], shfl_xor2(cp[2], 16));
+    const float2 u1 = add2(cp[1], shfl_xor2(cp[3], 16));
+    const float2 w = add2(u0, shfl_xor2(u1, 8));
+    const float keep = hi ? w.y : w.x, give = hi ? w.x : w.y;
+    float x = keep + __shfl_xor_sync(kAll, give, 4);
     x += __shfl_xor_sync(kAll, x, 2);
     x += __shfl_xor_sync(kAll, x, 1);
     return x;
 }
 
+template <int D, int R, int V, bool DO_S, bool MASK>
+__device__ __forceinline__ void sym_group_f32(const StagedTile<D>& t, int g, int q,
+                                              const Rows2<D, R>& w, const PairConsts& c,
+                                              float2 (&a)[R][kNumAcc],
+                                              float2 (&cp)[3][kSymGroup / 2]) {
+#pragma unroll
+    for (int m = 0; m < kSymGroup / 2; ++m) {
+        const int p = g / 2 + (m ^ q);
+        const int2 rj = MASK ? reinterpret_cast<const int2*>(t.rank)[p] : make_int2(0, 0);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            float2 d2, dt;
+            geometry2<D, R, V>(t, p, w, r, d2, dt);
+            const float2 t2 = mul2(dt, dt);
+            const float2 B = background2<V>(add2(d2, t2));
+            a[r][0] = add2(a[r][0], B);
+            a[r][1] = fma2(B, d2, a[r][1]);
+            a[r][2] = fma2(B, t2, a[r][2]);
+            if (r == 0) {
+                cp[0][m] = B;
+                cp[1][m] = mul2(B, d2);
+                cp[2][m] = mul2(B, t2);
+            } else {
+                cp[0][m] = add2(cp[0][m], B);
+                cp[1][m] = fma2(B, d2, cp[1][m]);
+                cp[2][m] = fma2(B, t2, cp[2][m]);
+            }
+            if (DO_S) {
+                const float2 S = self_excite2<V, MASK>(d2, dt, w.rk[r], rj, c);
+                a[r][3] = add2(a[r][3], S);
+                a[r][4] = fma2(S, d2, a[r][4]);
+                a[r][5] = fma2(S, dt, a[r][5]);
+            }
+        }
+    }
+}
+
 // One full tile J (kTile columns, all real events) before the strip.
 // sCol: [kSweepThreads / 32][3][kTile] floats of shared memory.
 template <int D, int R, int V, bool DO_S, bool MASK>
-__device__ __forceinline__ void tile_sym_f32(const float* __restrict__ sRec,
-                                             const float (&xh)[R][D], const float (&xl)[R][D],
-                                             const float (&th)[R], const float (&tl)[R],
-                                             const int (&rk)[R], const PairConsts& c,
-                                             double (&acc)[R][kNumAcc], float* __restrict__ sCol,
+__device__ __forceinline__ void tile_sym_f32(const StagedTile<D>& t, const Rows2<D, R>& w,
+                                             const PairConsts& c, double (&acc)[R][kNumAcc],
+                                             float* __restrict__ sCol,
                                              unsigned long long* __restrict__ colAcc, int Npad,
                                              int j0) {
     static_assert(kSweepThreads == kTile, "one column per thread in the column flush");
     static_assert(kFlush % kSymGroup == 0 && kTile % kFlush == 0, "group sizes");
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
-    const int perm = lane >> 2;
+    const int q = (lane >> 3) & 3;
+    const bool hi = (lane >> 2) & 1;
     for (int jb = 0; jb < kTile; jb += kFlush) {
-        float a[R][kNumAcc];
-#pragma unroll
-        for (int r = 0; r < R; ++r)
-#pragma unroll
-            for (int q = 0; q < kNumAcc; ++q) a[r][q] = 0.0f;
+        float2 a[R][kNumAcc];
+        zero_rows<R>(a);
 #pragma unroll 1
         for (int g = jb; g < jb + kFlush; g += kSymGroup) {
-            float cp[kSymGroup][3];
-            sym_group_f32<D, R, V, DO_S, MASK>(sRec, g, perm, xh, xl, th, tl, rk, c, a, cp);
-            const float c0 = sym_exchange(cp, 0);
-            const float c1 = sym_exchange(cp, 1);
-            const float c2 = sym_exchange(cp, 2);
+            float2 cp[3][kSymGroup / 2];
+            sym_group_f32<D, R, V, DO_S, MASK>(t, g, q, w, c, a, cp);
+            const float c0 = sym_exchange(cp[0], hi);
+            const float c1 = sym_exchange(cp[1], hi);
+            const float c2 = sym_exchange(cp[2], hi);
             if ((lane & 3) == 0) {
-                float* o = sCol + warp * 3 * kTile + g + perm;
+                float* o = sCol + warp * 3 * kTile + g + (lane >> 2);
                 o[0] = c0;
                 o[kTile] = c1;
                 o[2 * kTile] = c2;
             }
         }
-#pragma unroll
-        for (int r = 0; r < R; ++r)
-#pragma unroll
-            for (int q = 0; q < kNumAcc; ++q) acc[r][q] += (double)a[r][q];
+        flush_rows<R>(a, acc);
     }
     __syncthreads();
 #pragma unroll
-    for (int q = 0; q < 3; ++q) {
+    for (int qq = 0; qq < 3; ++qq) {
         double v = 0.0;
 #pragma unroll
-        for (int w = 0; w < kSweepThreads / 32; ++w) v += (double)sCol[(w * 3 + q) * kTile + tid];
-        atomicAdd(colAcc + (size_t)q * Npad + j0 + tid,
+        for (int wq = 0; wq < kSweepThreads / 32; ++wq)
+            v += (double)sCol[(wq * 3 + qq) * kTile + tid];
+        atomicAdd(colAcc + (size_t)qq * Npad + j0 + tid,
                   (unsigned long long)__double2ll_rn(v * kColScale));
     }
 }
@@ -590,15 +760,14 @@ __device__ __forceinline__ void f32c_item(const float* __restrict__ rec,
                                           double* __restrict__ partials,
                                           unsigned long long* __restrict__ colAcc, int N,
                                           int nTiles, int Npad, bool sym, const PairConsts& c,
-                                          int strip, int jt0, int jt1, int slot, float* sRec,
-                                          float* sCol) {
+                                          int strip, int jt0, int jt1, int slot,
+                                          StagedTile<D>& st, float* sCol) {
     constexpr int S = Layout<D>::kF32Stride;
     const int tid = threadIdx.x;
     const int stripBase = strip * kSweepThreads * R;
     const int ts0 = stripBase / kTile, ts1 = min(ts0 + R, nTiles);
 
-    float xh[R][D], xl[R][D], th[R], tl[R];
-    int rk[R];
+    Rows2<D, R> w;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const int iRaw = stripBase + r * kSweepThreads + tid;
@@ -606,18 +775,18 @@ __device__ __forceinline__ void f32c_item(const float* __restrict__ rec,
         const float* ri = rec + (size_t)i * S;
 #pragma unroll
         for (int k = 0; k < D; ++k) {
-            xh[r][k] = ri[k];
-            xl[r][k] = ri[D + 1 + k];
+            w.xh[r][k] = dup2(ri[k]);
+            w.xl[r][k] = dup2(ri[D + 1 + k]);
         }
-        th[r] = ri[D];
-        tl[r] = ri[2 * D + 1];
-        rk[r] = __float_as_int(ri[2 * D + 2]);
+        w.th[r] = dup2(ri[D]);
+        w.tl[r] = dup2(ri[2 * D + 1]);
+        w.rk[r] = __float_as_int(ri[2 * D + 2]);
         if (iRaw >= N) {
             // Padding rows of the last strip: a time 1e18 away makes every
             // background term exactly +0 (exponent ~ -1e36, finite), so they
             // add nothing to the column sums; their own rows are discarded.
-            th[r] = 1e18f;
-            tl[r] = 0.0f;
+            w.th[r] = dup2(1e18f);
+            w.tl[r] = dup2(0.0f);
         }
     }
     double tminI = INFINITY, tmaxI = -INFINITY;
@@ -642,33 +811,49 @@ __device__ __forceinline__ void f32c_item(const float* __restrict__ rec,
         const int j0 = jt * kTile;
         const int nj = min(kTile, N - j0);
         __syncthreads();
-        const float4* src = reinterpret_cast<const float4*>(rec + (size_t)j0 * S);
-        float4* dst = reinterpret_cast<float4*>(sRec);
-        for (int v = tid; v < nj * (S / 4); v += kSweepThreads) dst[v] = src[v];
+        // stage the tile: one thread per column, fields negated
+        if (tid < nj) {
+            const float* rj = rec + (size_t)(j0 + tid) * S;
+#pragma unroll
+            for (int k = 0; k < D; ++k) {
+                st.nx[k][tid] = -rj[k];
+                st.nxl[k][tid] = -rj[D + 1 + k];
+            }
+            st.nt[tid] = -rj[D];
+            st.ntl[tid] = -rj[2 * D + 1];
+            st.rank[tid] = __float_as_int(rj[2 * D + 2]);
+        } else if (tid == nj && (nj & 1)) {
+            // padding column of an odd tile: coordinate and time 1e18 away
+#pragma unroll
+            for (int k = 0; k < D; ++k) {
+                st.nx[k][tid] = -1e18f;
+                st.nxl[k][tid] = 0.0f;
+            }
+            st.nt[tid] = 1e18f;
+            st.ntl[tid] = 0.0f;
+            st.rank[tid] = INT_MAX;
+        }
         __syncthreads();
         if (sym && m.doB && jt < ts0) {
             // jt < ts0 <= nTiles - 1: a full tile
             if (!m.doS)
-                tile_sym_f32<D, R, V, false, false>(sRec, xh, xl, th, tl, rk, c, acc, sCol,
-                                                    colAcc, Npad, j0);
+                tile_sym_f32<D, R, V, false, false>(st, w, c, acc, sCol, colAcc, Npad, j0);
             else if (m.allCausal)
-                tile_sym_f32<D, R, V, true, false>(sRec, xh, xl, th, tl, rk, c, acc, sCol, colAcc,
-                                                   Npad, j0);
+                tile_sym_f32<D, R, V, true, false>(st, w, c, acc, sCol, colAcc, Npad, j0);
             else
-                tile_sym_f32<D, R, V, true, true>(sRec, xh, xl, th, tl, rk, c, acc, sCol, colAcc,
-                                                  Npad, j0);
+                tile_sym_f32<D, R, V, true, true>(st, w, c, acc, sCol, colAcc, Npad, j0);
         } else if (m.doB) {
             if (!m.doS)
-                tile_f32<D, R, V, true, false, false>(sRec, nj, xh, xl, th, tl, rk, c, acc);
+                tile_f32<D, R, V, true, false, false>(st, nj, w, c, acc);
             else if (m.allCausal)
-                tile_f32<D, R, V, true, true, false>(sRec, nj, xh, xl, th, tl, rk, c, acc);
+                tile_f32<D, R, V, true, true, false>(st, nj, w, c, acc);
             else
-                tile_f32<D, R, V, true, true, true>(sRec, nj, xh, xl, th, tl, rk, c, acc);
+                tile_f32<D, R, V, true, true, true>(st, nj, w, c, acc);
         } else {
             if (m.allCausal)
-                tile_f32<D, R, V, false, true, false>(sRec, nj, xh, xl, th, tl, rk, c, acc);
+                tile_f32<D, R, V, false, true, false>(st, nj, w, c, acc);
             else
-                tile_f32<D, R, V, false, true, true>(sRec, nj, xh, xl, th, tl, rk, c, acc);
+                tile_f32<D, R, V, false, true, true>(st, nj, w, c, acc);
         }
     }
 #pragma unroll
@@ -689,7 +874,7 @@ __global__ void __launch_bounds__(kSweepThreads, (R <= 2 ? 4 : 2))
 sweep_f32c_list_kernel(const SweepProblem* __restrict__ problems,
                        const WorkItem* __restrict__ items, const int* __restrict__ nItems,
                        int* __restrict__ counter) {
-    __shared__ __align__(16) float sRec[kTile * Layout<D>::kF32Stride];
+    __shared__ __align__(16) StagedTile<D> sTile;
     __shared__ __align__(16) float sCol[(kSweepThreads / 32) * 3 * kTile];
     __shared__ int sNext;
     const int n = *nItems;
@@ -701,7 +886,7 @@ sweep_f32c_list_kernel(const SweepProblem* __restrict__ problems,
         const PairConsts c = P.c;
         f32c_item<D, R, V>(static_cast<const float*>(P.rec), P.tileMin, P.tileMax, P.partials,
                            P.colAcc, P.N, P.nTiles, P.Npad, P.symmetric != 0, c, w.strip, w.jt0,
-                           w.jt1, w.slot, sRec, sCol);
+                           w.jt1, w.slot, sTile, sCol);
     }
 }
 
@@ -840,7 +1025,14 @@ finish_list_kernel(const FinishProblem* __restrict__ problems,
             double acc = 0.0;
             for (int ch = 0; ch < nc; ++ch)
                 acc += P.partials[((size_t)ch * kNumAcc + q) * P.Npad + i];
-            if (q < 3 && P.colAcc) acc += (double)P.colAcc[(size_t)q * P.Npad + i] * kColInv;
+            if (q < 3 && P.colAcc) {
+                if (P.colWords == 2)  // FP64 sweep: two-word fixed point
+                    acc += ldexp((double)P.colAcc[(size_t)(2 * q) * P.Npad + i], -P.colShift[q]) +
+                           ldexp((double)P.colAcc[(size_t)(2 * q + 1) * P.Npad + i],
+                                 -(P.colShift[q] + kColLoBits));
+                else
+                    acc += (double)P.colAcc[(size_t)q * P.Npad + i] * kColInv;
+            }
             s[q] = acc * f.accScale[q];
             if (P.sums) P.sums[(size_t)q * N + i] = s[q];
         }

@@ -43,11 +43,6 @@ struct PairConsts {
     // S exponent (log2 units) = kS |dx'|^2 + kW dt' with kS = -sigma^2 / a^2 and
     // kW = -omega log2(e) / sT, each split hi + lo.
     float fSh, fSl, fWh, fWl;
-    // Added to every FP32 exponent: -log2(1 + beta), where beta is the mean
-    // relative error of ex2.approx.ftz.f32 measured on the device at engine
-    // creation (the instruction rounds low on average), so the FP32 pair
-    // terms carry no common bias into the sums.
-    float ex2Fix;
     // Tile-pair underflow skips.  A tile pair is skipped for B when every B_u
     // in it is exactly zero in the working precision: cA <= 0, cB < 0 and
     // -cB * min|dt|^2 >= skipB.  Likewise for S with -cW * min(dt) >= skipS.
@@ -61,7 +56,9 @@ struct FinishConsts {
     double prefS;     // theta omega sigma^D / sqrt(2 pi) : S_ij = prefS * S_u
     double bgScale;   // prefB / mu0
     double seScale;   // prefS / theta
-    double accScale[6];  // multiplies the six unit pair sums (undoes the record scaling)
+    double accScale[6];  // multiplies the six unit pair sums: undoes the record scaling
+                         // and, with the hardware exponential, divides out its mean
+                         // relative error (1 + beta, measured on the device)
     double T;         // t[N-1]
     double constant;  // N (D-1) log(1/sqrt(2 pi))
     int D;
@@ -129,6 +126,12 @@ inline int finish_blocks(int N) { return (N + kFinishThreads - 1) / kFinishThrea
 constexpr double kColScale = 68719476736.0;
 constexpr double kColInv = 1.0 / 68719476736.0;
 constexpr int kMaxSymmetricEvents = 1 << 27;
+// FP64 symmetric sweep: each column sum is two unsigned 64-bit words, hi in
+// units of 2^-colShift[q] and lo in units of 2^-(colShift[q] + kColLoBits),
+// the shift chosen per problem so that a column total stays below 2^62
+// units of hi (resolution of the pair ~2^-(colShift + 40), far below FP64
+// rounding of the sums).
+constexpr int kColLoBits = 40;
 
 // Pair-sweep view of a problem.
 //
@@ -143,8 +146,10 @@ struct SweepProblem {
     const double* tileMin;  // per kTile-event tile of the problem's set
     const double* tileMax;
     double* partials;       // [slot][6][Npad]
-    unsigned long long* colAcc;  // [3][Npad] background column sums x kColScale, or null
+    unsigned long long* colAcc;  // background column sums, or null: FP32 [3][Npad] x kColScale;
+                                 // FP64 [3][2][Npad] two-word fixed point (see kColLoBits)
     int N, nTiles, Npad, symmetric;
+    int colShift[4];        // FP64 column sums: fixed-point shift per weighted sum
     PairConsts c;
 };
 
@@ -166,7 +171,8 @@ struct FinishProblem {
     double* probs;            // P_i output (may be null)
     double* sums;             // [6][N] unit pair sums out, natural units (may be null)
     int N, Npad, stripEvents, blockBase;  // blockBase: first finish CTA of this problem
-    int nBlocks, pad0, pad1, pad2;
+    int nBlocks, colWords, pad0, pad1;    // colWords: 1 = FP32 column format, 2 = FP64
+    int colShift[4];
     FinishConsts f;
 };
 

@@ -159,7 +159,6 @@ extern "C" int hphc_loglik_grad_fp64_static(int embeddingDimension, int location
     c.cB = -0.5 * b * b;
     c.cS = -0.5 * sigma * sigma;
     c.cW = -omega;
-    c.ex2Fix = 0.0f;
     const double kSkip = 760.0;  // FP64 exp(x) is +0 below -745.2
     c.skipB = (c.cB < 0.0) ? kSkip : -1.0;
     c.skipS = (c.cW < 0.0) ? kSkip : -1.0;

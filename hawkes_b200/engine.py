@@ -46,7 +46,8 @@ COMPENSATED = 1 << 9
 NO_UNDERFLOW_SKIP = 1 << 10
 FP32_FAST_EXP = 1 << 11
 FP32_SPACE_HILO = 1 << 12
-FP32_ORDERED = 1 << 13
+ORDERED = 1 << 13       # both orders of every background pair, either precision
+FP32_ORDERED = ORDERED  # earlier name of the same bit
 NO_INCREMENTAL = 1 << 14
 
 # How an evaluation was computed (CudaHawkes.lastEvaluationPath).

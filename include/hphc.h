@@ -69,9 +69,11 @@ extern "C" {
                                                 components lose accuracy (~1e-6) */
 #define HPHC_FLAG_FP32_SPACE_HILO (1L << 12) /* coordinate differences from hi/lo float
                                                 pairs (times always use hi/lo pairs) */
-#define HPHC_FLAG_FP32_ORDERED (1L << 13)    /* evaluate both orders of every background
-                                                pair (by default each pair is evaluated
-                                                once and added to both events' sums) */
+#define HPHC_FLAG_ORDERED (1L << 13)         /* evaluate both orders of every background
+                                                pair, in either precision (by default each
+                                                pair is evaluated once and added to both
+                                                events' sums) */
+#define HPHC_FLAG_FP32_ORDERED HPHC_FLAG_ORDERED /* earlier name of the same bit */
 #define HPHC_FLAG_NO_INCREMENTAL (1L << 14)  /* always run the full pair sweep (by default
                                                 an evaluation at unchanged parameters after
                                                 a few single-event updateLocations calls

@@ -26,13 +26,15 @@ pytestmark = pytest.mark.gpu
 FP64 = hb.CUDA
 FP32C = hb.CUDA | hb.COMPENSATED
 FP32F = hb.CUDA | hb.COMPENSATED | hb.FP32_FAST_EXP
-FP32O = hb.CUDA | hb.COMPENSATED | hb.FP32_ORDERED
+FP32O = hb.CUDA | hb.COMPENSATED | hb.ORDERED
+FP64O = hb.CUDA | hb.ORDERED
 TOL = {FP64: dict(ll=1e-10, grad=1e-10, probs=1e-10),
+       FP64O: dict(ll=1e-10, grad=1e-10, probs=1e-10),
        FP32C: dict(ll=1e-7, grad=5e-6, probs=2e-5),
        FP32F: dict(ll=1e-7, grad=5e-6, probs=2e-5),
        FP32O: dict(ll=1e-7, grad=5e-6, probs=2e-5)}
-MODES = [FP64, FP32C, FP32F, FP32O]
-IDS = ["fp64", "fp32c", "fp32c_fast", "fp32c_ordered"]
+MODES = [FP64, FP64O, FP32C, FP32F, FP32O]
+IDS = ["fp64", "fp64_ordered", "fp32c", "fp32c_fast", "fp32c_ordered"]
 
 
 def engine(loc, t, p, flags):
@@ -56,10 +58,11 @@ def check_case(name, c, flags):
     assert ll == ll2 and np.array_equal(g, g2), name
     # FP64: against the per-event scale; FP32: against the term-level scale
     # (the condition scale of the sum, which is what FP32 pair terms resolve)
-    key = "grad_scale" if flags == FP64 else "grad_term_scale"
+    fp64 = flags in (FP64, FP64O)
+    key = "grad_scale" if fp64 else "grad_term_scale"
     scale = np.maximum(c[key], 1e-300)
     allowed = tol["grad"] * scale
-    if flags != FP64:
+    if not fp64:
         # An FP32 exponent e (log2 units, |e| <= 126) carries an absolute
         # error ~|e| 2^-23, so a pair term far out in its kernel is resolved
         # only to ~1e-6 relative, and terms below 2^-126 flush to zero.  A
@@ -120,12 +123,13 @@ def test_unsorted_times_against_oracle(flags):
         check_case(f"unsorted_D{D}_N{N}", c, flags)
 
 
-def test_symmetric_sweep_halves_background_work():
+@pytest.mark.parametrize("sym,ordered", [(FP32C, FP32O), (FP64, FP64O)], ids=["fp32c", "fp64"])
+def test_symmetric_sweep_halves_background_work(sym, ordered):
     # Each background pair with an earlier tile is evaluated once for both
     # events: the same terms are accounted for with about half the exponentials.
     loc, t = workloads.uniform(30000, seed=21)
     p = workloads.BASE_PARAMS
-    with engine(loc, t, p, FP32C) as s, engine(loc, t, p, FP32O) as o:
+    with engine(loc, t, p, sym) as s, engine(loc, t, p, ordered) as o:
         for e in (s, o):
             e.setSweepShape(2, 16)
         ls, gs = s.getLogLikelihoodAndGradient()
@@ -138,6 +142,9 @@ def test_symmetric_sweep_halves_background_work():
     # for slightly different sets of exactly-zero terms.
     assert abs(nbs - nbo) <= 0.01 * nbo and nss == nso
     assert evo == nbo and evs < 0.55 * evo
+    if sym == FP64:  # the FP64 column sums are exact to FP64 rounding
+        assert abs(ls - lo) <= 1e-13 * abs(lo)
+        assert np.all(np.abs(gs - go) <= 1e-11 * (np.abs(go) + 1.0))
     assert abs(ls - lo) <= 1e-9 * abs(lo)
 
 
