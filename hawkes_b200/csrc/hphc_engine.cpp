@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -194,36 +195,44 @@ struct EventSet {
 
     // Host-side derived data of the times: sortedness, dense ranks (equal
     // times share a rank: the exact strict-causality mask of the FP32
-    // records), per-tile bounds.
+    // records), per-tile bounds.  Sorted times (the usual case) take one pass
+    // for sortedness and ranks, and the tile bounds are each tile's first and
+    // last time.
     void derive_times() {
-        sorted = true;
-        for (int i = 1; i < N && sorted; ++i) sorted = hTimes.p[i - 1] <= hTimes.p[i];
-        if (sorted) {
-            int r = 0;
-            for (int i = 0; i < N; ++i) {
-                if (i > 0 && hTimes.p[i] != hTimes.p[i - 1]) ++r;
-                hRanks.p[i] = r;
-            }
-        } else {
-            std::vector<int> idx(N);
-            std::iota(idx.begin(), idx.end(), 0);
-            std::stable_sort(idx.begin(), idx.end(),
-                             [&](int x, int y) { return hTimes.p[x] < hTimes.p[y]; });
-            int r = 0;
-            for (int k = 0; k < N; ++k) {
-                if (k > 0 && hTimes.p[idx[k]] != hTimes.p[idx[k - 1]]) ++r;
-                hRanks.p[idx[k]] = r;
-            }
+        const double* t = hTimes.p;
+        bool asc = true;
+        int r = 0;
+        hRanks.p[0] = 0;
+        for (int i = 1; i < N; ++i) {
+            asc &= t[i - 1] <= t[i];
+            r += t[i] != t[i - 1];
+            hRanks.p[i] = r;
         }
+        sorted = asc;
         const int nTiles = (N + kTile - 1) / kTile;
-        for (int t = 0; t < nTiles; ++t) {
-            double lo = INFINITY, hi = -INFINITY;
-            for (int j = t * kTile; j < std::min(N, (t + 1) * kTile); ++j) {
-                lo = std::min(lo, hTimes.p[j]);
-                hi = std::max(hi, hTimes.p[j]);
+        if (sorted) {
+            for (int k = 0; k < nTiles; ++k) {
+                hTileMin[k] = t[k * kTile];
+                hTileMax[k] = t[std::min(N, (k + 1) * kTile) - 1];
             }
-            hTileMin[t] = lo;
-            hTileMax[t] = hi;
+            return;
+        }
+        std::vector<int> idx(N);
+        std::iota(idx.begin(), idx.end(), 0);
+        std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return t[x] < t[y]; });
+        r = 0;
+        for (int k = 0; k < N; ++k) {
+            if (k > 0 && t[idx[k]] != t[idx[k - 1]]) ++r;
+            hRanks.p[idx[k]] = r;
+        }
+        for (int k = 0; k < nTiles; ++k) {
+            double lo = INFINITY, hi = -INFINITY;
+            for (int j = k * kTile; j < std::min(N, (k + 1) * kTile); ++j) {
+                lo = std::min(lo, t[j]);
+                hi = std::max(hi, t[j]);
+            }
+            hTileMin[k] = lo;
+            hTileMax[k] = hi;
         }
     }
 
@@ -319,7 +328,18 @@ struct Runtime {
     }
 };
 
+// True if every entry is finite; otherwise *bad = the first that is not.  The
+// first pass tests the exponent bits (all ones for NaN and infinity) with a
+// branch-free reduction the compiler vectorises.
 bool all_finite(const double* v, size_t n, size_t* bad) {
+    constexpr uint64_t kExp = 0x7ff0000000000000ULL;
+    uint64_t any = 0;
+    for (size_t i = 0; i < n; ++i) {
+        uint64_t u;
+        std::memcpy(&u, v + i, sizeof u);
+        any |= (uint64_t)((u & kExp) == kExp);
+    }
+    if (!any) return true;
     for (size_t i = 0; i < n; ++i)
         if (!std::isfinite(v[i])) {
             *bad = i;

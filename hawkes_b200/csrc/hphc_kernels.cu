@@ -54,30 +54,6 @@ __global__ void pack_f64_kernel(int N, const double* __restrict__ loc,
     for (int k = D + 1; k < S; ++k) r[k] = 0.0;
 }
 
-template <int D>
-__global__ void pack_f32_kernel(int N, const double* __restrict__ loc,
-                                const double* __restrict__ times, const int32_t* __restrict__ ranks,
-                                double sX, double sT, float* __restrict__ rec) {
-    constexpr int S = Layout<D>::kF32Stride;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= N) return;
-    float* r = rec + (size_t)i * S;
-#pragma unroll
-    for (int k = 0; k < D; ++k) {
-        const double v = loc[(size_t)i * D + k] * sX;
-        const float h = (float)v;
-        r[k] = h;
-        r[D + 1 + k] = (float)(v - (double)h);
-    }
-    const double v = times[i] * sT;
-    const float h = (float)v;
-    r[D] = h;
-    r[2 * D + 1] = (float)(v - (double)h);
-    r[2 * D + 2] = __int_as_float(ranks[i]);
-#pragma unroll
-    for (int k = 2 * D + 3; k < S; ++k) r[k] = 0.0f;
-}
-
 // FP32 records for many problems in one launch: blockIdx.y = job.
 template <int D>
 __global__ void pack_f32_jobs_kernel(const PackJob* __restrict__ jobs) {
@@ -1177,20 +1153,6 @@ cudaError_t launch_pack_f64(int D, int N, const double* loc, const double* times
         default: return cudaErrorInvalidValue;
     }
     tile_bounds_kernel<<<(N + kTile - 1) / kTile, kTile, 0, s>>>(N, times, tileMin, tileMax);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_pack_f32(int D, int N, const double* loc, const double* times,
-                            const int32_t* ranks, double sX, double sT, float* rec,
-                            cudaStream_t s) {
-    const int blocks = (N + 255) / 256;
-    switch (D) {
-#define X(d) \
-    case d: pack_f32_kernel<d><<<blocks, 256, 0, s>>>(N, loc, times, ranks, sX, sT, rec); break;
-        HPHC_FOR_EACH_DIM(X)
-#undef X
-        default: return cudaErrorInvalidValue;
-    }
     return cudaGetLastError();
 }
 

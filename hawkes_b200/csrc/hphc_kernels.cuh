@@ -79,11 +79,6 @@ struct SweepGeometry {
 // compute per-tile time bounds.  ranks may be null for the FP64 layout.
 cudaError_t launch_pack_f64(int D, int N, const double* loc, const double* times, double* rec,
                             double* tileMin, double* tileMax, cudaStream_t s);
-// FP32 records of coordinates scaled by sX and times scaled by sT (no tile
-// bounds: those come from launch_tile_bounds).
-cudaError_t launch_pack_f32(int D, int N, const double* loc, const double* times,
-                            const int32_t* ranks, double sX, double sT, float* rec,
-                            cudaStream_t s);
 cudaError_t launch_tile_bounds(int N, const double* times, double* tileMin, double* tileMax,
                                cudaStream_t s);
 

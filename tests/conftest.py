@@ -34,3 +34,15 @@ def golden_synthetic():
 @pytest.fixture(scope="session")
 def golden_dcdata():
     return load_golden("dcdata.npz")
+
+
+@pytest.fixture(scope="session")
+def events_50k():
+    """The accuracy workload: N = 50,000 uniform events (seed 1), base
+    parameters, and the oracle's log-likelihood, gradient and scales."""
+    import oracle
+    from hawkes_b200 import workloads
+    loc, t = workloads.uniform(50000, seed=1)
+    p = workloads.BASE_PARAMS.copy()
+    o = oracle.oracle_eval(loc, t, p, threads=max(1, os.cpu_count() or 1))
+    return loc, t, p, o

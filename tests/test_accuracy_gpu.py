@@ -26,11 +26,8 @@ N = 50000
 
 
 @pytest.fixture(scope="module")
-def c2():
-    loc, t = workloads.uniform(N, seed=1)
-    p = workloads.BASE_PARAMS.copy()
-    o = oracle.oracle_eval(loc, t, p, threads=max(1, os.cpu_count() or 1))
-    return loc, t, p, o
+def c2(events_50k):
+    return events_50k
 
 
 def run(loc, t, p, flags):
