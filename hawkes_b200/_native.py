@@ -75,6 +75,8 @@ SIGNATURES = {
     "hphc_sampler_last_error": (ctypes.c_char_p, [_handle]),
     "hphc_sampler_run": (ctypes.c_int, [_handle, _handle, ctypes.c_int, ctypes.c_int, _c_double_p,
                                         _c_double_p]),
+    "hphc_sampler_run_device": (ctypes.c_int, [_handle, _handle, ctypes.c_int, ctypes.c_int,
+                                               _c_double_p, _c_double_p]),
     "hphc_sampler_run_with": (ctypes.c_int, [_handle, ctypes.c_void_p, ctypes.c_void_p,
                                              ctypes.c_int, ctypes.c_int, _c_double_p,
                                              _c_double_p]),

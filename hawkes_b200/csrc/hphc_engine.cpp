@@ -30,6 +30,7 @@
 
 #include "hphc.h"
 #include "hphc_executor.h"
+#include "hphc_internal.h"
 #include "hphc_kernels.cuh"
 
 using namespace hphc;
@@ -619,6 +620,26 @@ struct hphc_multiset {
         for (auto& h : hLoc) h.release();
     }
 };
+
+int hphc::engine_loop_setup(hphc_engine* e, const double* params, int K, EngineLoop* out,
+                            std::string* err) {
+    DeviceGuard g(e->rt.device);
+    if (!g.ok) return fmt(*err, HPHC_ERR_CUDA, "cannot select device %d", e->rt.device);
+    // moved events are only on the host, and after incremental row uploads
+    // the packed FP64 records are stale: upload and pack everything
+    if (!e->moved.empty() || e->recStale) e->dirty = true;
+    int st = e->upload_if_dirty();
+    if (st) return fmt(*err, st, "%s", e->lastError.c_str());
+    std::vector<SetView> sets{e->set.view()};
+    std::vector<int> setOf(K, 0);
+    st = e->rt.ex.setup_device_loop(sets, setOf.data(), params, K);
+    if (st) return fmt(*err, st, "%s", e->rt.ex.error.c_str());
+    out->device = e->rt.device;
+    out->stream = e->rt.stream;
+    out->ex = &e->rt.ex;
+    out->spec = e->rt.ex.consts_spec();
+    return HPHC_OK;
+}
 
 // ------------------------------------------------------------------ C ABI --
 

@@ -15,22 +15,9 @@ namespace {
 
 constexpr double kInvSqrt2Pi = 0.398942280401432677939946059934;
 constexpr double kLog2e = 1.44269504088896340735992468100189214;
-constexpr double kTwoPi = 6.28318530717958647692528676655900577;
 
-// Underflow thresholds (natural-log units) for the tile-pair skip.  FP32:
-// both exponentials return +0 for any argument below -126.5 (log2 units); a
-// true exponent <= -88 is <= -126.96 in log2 units, which the FP32 rounding
-// of the computed exponent (relative ~1e-6) cannot lift above -126.5.  FP64:
-// exp(x) is +0 for x < -745.14; -760 leaves a wide margin.
-constexpr double kSkipF32 = 88.0;
-constexpr double kSkipF64 = 760.0;
 
 size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
-
-void split_float(double x, float& hi, float& lo) {
-    hi = (float)x;
-    lo = (float)(x - (double)hi);
-}
 
 double record_scale(double precisionParam) {
     return std::fabs(precisionParam) * std::sqrt(0.5 * kLog2e);
@@ -118,49 +105,30 @@ void Executor::release() {
     for (auto& ev : ev_) ev = nullptr;
 }
 
+ConstsSpec Executor::consts_spec() const {
+    ConstsSpec s{};
+    s.precision = precision_ == HPHC_PRECISION_FP64 ? 0 : 1;
+    s.D = D_;
+    s.variant = variant_;
+    s.skip = skip_ ? 1 : 0;
+    s.ex2Bias = ex2Bias_;
+    return s;
+}
+
 PairConsts Executor::pair_consts(const double* p) const {
-    const double sigma = p[0], a = p[1], b = p[2], omega = p[3];
     PairConsts c{};
-    c.cA = -0.5 * a * a;
-    c.cB = -0.5 * b * b;
-    c.cS = -0.5 * sigma * sigma;
-    c.cW = -omega;
-    if (precision_ != HPHC_PRECISION_FP64) {
-        const double sT = record_scale(b);
-        split_float(-(sigma * sigma) / (a * a), c.fSh, c.fSl);
-        split_float(-omega * kLog2e / sT, c.fWh, c.fWl);
-    }
-    const double thr = precision_ == HPHC_PRECISION_FP64 ? kSkipF64 : kSkipF32;
-    c.skipB = (skip_ && c.cB < 0.0 && c.cA <= 0.0) ? thr : -1.0;
-    c.skipS = (skip_ && c.cW < 0.0 && c.cS <= 0.0) ? thr : -1.0;
+    FinishConsts f{};
+    param_consts(p, consts_spec(), c, f);
     return c;
 }
 
 FinishConsts Executor::finish_consts(const double* p, const SetView& set) const {
+    PairConsts c{};
     FinishConsts f{};
-    f.sigma = p[0];
-    f.a = p[1];
-    f.b = p[2];
-    f.omega = p[3];
-    f.theta = p[4];
-    f.mu0 = p[5];
-    f.bgScale = std::pow(f.a, D_) * f.b / kTwoPi;
-    f.seScale = f.omega * std::pow(f.sigma, D_) * kInvSqrt2Pi;
-    f.prefB = f.mu0 * f.bgScale;
-    f.prefS = f.theta * f.seScale;
-    for (int q = 0; q < kNumAcc; ++q) f.accScale[q] = 1.0;
-    if (precision_ != HPHC_PRECISION_FP64) {
-        const double sX = record_scale(f.a), sT = record_scale(f.b);
-        f.accScale[1] = f.accScale[4] = 1.0 / (sX * sX);  // sums of d'^2
-        f.accScale[2] = 1.0 / (sT * sT);                  // sum of dt'^2
-        f.accScale[5] = 1.0 / sT;                         // sum of dt'
-        if (!(variant_ & 2))  // hardware exponential: divide out its mean relative error
-            for (int q = 0; q < kNumAcc; ++q) f.accScale[q] /= 1.0 + ex2Bias_;
-    }
+    param_consts(p, consts_spec(), c, f);
     f.T = set.hTimes[set.N - 1];
     // src/NewHawkes.hpp:659: locationCount * (embeddingDimension - 1) * log(M_1_SQRT_2PI)
     f.constant = (double)(set.N * (D_ - 1)) * std::log(kInvSqrt2Pi);
-    f.D = D_;
     return f;
 }
 
@@ -274,7 +242,27 @@ int Executor::build_plan(const std::vector<SetView>& sets, const int* setOf, con
                 tmaxI = std::max(tmaxI, s.hTileMax[t]);
             }
             int lo = 0, hi = nTiles;
-            if (s.sorted) {
+            if (s.sorted && wideBands_) {
+                // any sampled sigma, omega: every earlier tile may hold
+                // self-excitation terms; the background band (tauT fixed)
+                // is as below
+                auto neededB = [&](int jt) {
+                    bool b, se;
+                    tile_needs(tminI, tmaxI, s.hTileMin[jt], s.hTileMax[jt], sp.c, &b, &se);
+                    return b;
+                };
+                lo = 0;
+                if (sp.symmetric) {
+                    hi = ts1;
+                } else {
+                    int a = ts1, b = nTiles;
+                    while (a < b) {
+                        const int m = (a + b) / 2;
+                        if (neededB(m)) a = m + 1; else b = m;
+                    }
+                    hi = std::min(nTiles, a + 1);
+                }
+            } else if (s.sorted) {
                 auto needed = [&](int jt) {
                     bool b, se;
                     tile_needs(tminI, tmaxI, s.hTileMin[jt], s.hTileMax[jt], sp.c, &b, &se);
@@ -636,6 +624,73 @@ int Executor::wait(double* hostOut) {
         }
     }
     return HPHC_OK;
+}
+
+int Executor::setup_device_loop(const std::vector<SetView>& sets, const int* setOf,
+                                const double* params, int P) {
+    if (P < 1) {
+        error = "no problems to evaluate";
+        return HPHC_ERR_BAD_ARGUMENT;
+    }
+    if (fixedR && fixedItems) {
+        R = fixedR;
+        itemsPerSM = fixedItems;
+        tuned_ = true;
+    }
+    if (!tuned_) {
+        const int st = autotune(sets, setOf, params, P, nullptr);
+        if (st) return st;
+    }
+    wideBands_ = true;
+    int st = build_plan(sets, setOf, params, P, nullptr, R, itemsPerSM);
+    wideBands_ = false;
+    if (st) return st;
+    drop_graph();  // the tables' layout changed under any captured graph
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(dTables_, hStaging_, tablesBytes_, cudaMemcpyHostToDevice, stream_)))
+        return cuda_fail(e, "stage tables");
+    if (precision_ != HPHC_PRECISION_FP64) {
+        char* d = static_cast<char*>(dTables_);
+        if ((e = launch_pack_f32_jobs(D_, plan_.P, plan_.maxN,
+                                      reinterpret_cast<const PackJob*>(d + offPJ_), stream_)))
+            return cuda_fail(e, "pack kernel");
+    }
+    if ((e = cudaStreamSynchronize(stream_))) return cuda_fail(e, "device loop set-up");
+    loopGrid_ = sweep_grid(R);
+    return HPHC_OK;
+}
+
+int Executor::enqueue_device_body() {
+    const int prec = precision_ == HPHC_PRECISION_FP64 ? 0 : 1;
+    char* d = static_cast<char*>(dTables_);
+    const auto* sp = reinterpret_cast<const SweepProblem*>(d + offSP_);
+    const auto* items = reinterpret_cast<const WorkItem*>(d + offItems_);
+    const auto* nItems = reinterpret_cast<const int*>(d + offNItems_);
+    const auto* fp = reinterpret_cast<const FinishProblem*>(d + offFP_);
+    const auto* fb = reinterpret_cast<const FinishBlock*>(d + offFB_);
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(dCounter_, 0, sizeof(int), stream_)))
+        return cuda_fail(e, "reset work counter");
+    if (colNeed_ && (e = cudaMemsetAsync(dColAcc_, 0, colNeed_ * sizeof(unsigned long long),
+                                         stream_)))
+        return cuda_fail(e, "reset column sums");
+    if ((e = launch_sweep_list(prec, D_, R, variant_, loopGrid_, sp, items, nItems, dCounter_,
+                               stream_)))
+        return cuda_fail(e, "sweep kernel");
+    if ((e = launch_finish_list(plan_.nBlocks, fp, fb, dBlockSums_, stream_)))
+        return cuda_fail(e, "finish kernel");
+    if ((e = launch_final_list(plan_.P, fp, dBlockSums_, dOut_, stream_)))
+        return cuda_fail(e, "final kernel");
+    lastLaunches = 3;
+    return HPHC_OK;
+}
+
+SweepProblem* Executor::device_sweep_problems() const {
+    return reinterpret_cast<SweepProblem*>(static_cast<char*>(dTables_) + offSP_);
+}
+
+FinishProblem* Executor::device_finish_problems() const {
+    return reinterpret_cast<FinishProblem*>(static_cast<char*>(dTables_) + offFP_);
 }
 
 void Executor::count_terms(const std::vector<SetView>& sets, double* bTerms, double* sTerms,

@@ -64,6 +64,22 @@ public:
     // gradient, 0) to hostOut.
     int wait(double* hostOut);
 
+    // Device-resident loop (the on-device sampler): build the plan for P
+    // problems once, with bands wide enough for any sigma, omega, theta and
+    // mu0 at the problems' own tauX and tauT (all earlier tiles of sorted
+    // times; the kernel still skips tile pairs whose terms all underflow),
+    // upload its tables and pack the FP32 records.  enqueue_device_body()
+    // then runs sweep, finish and final on those device tables, whose
+    // per-problem constants a device kernel may rewrite between runs; the
+    // P x 8 results are at device_results().  A later enqueue() replaces the
+    // tables.
+    int setup_device_loop(const std::vector<SetView>& sets, const int* setOf,
+                          const double* params, int P);
+    int enqueue_device_body();
+    SweepProblem* device_sweep_problems() const;
+    FinishProblem* device_finish_problems() const;
+    const double* device_results() const { return dOut_; }
+
     // Pair terms the last run's sweep accounted for (replays the tile
     // decisions): background terms (both orders of a symmetric pair),
     // self-excitation terms, and background exponentials evaluated.
@@ -84,6 +100,8 @@ public:
 private:
     int D_ = 0, precision_ = 0, variant_ = 0, device_ = 0, numSMs_ = 148;
     bool skip_ = true;
+    bool wideBands_ = false;  // build_plan: bands for any sampled parameters
+    int loopGrid_ = 0;        // sweep grid of the device loop
     double ex2Bias_ = 0.0;
     cudaStream_t stream_ = nullptr;
     bool tuned_ = false;
@@ -148,6 +166,7 @@ private:
     bool capturing_ = false;
 
 public:
+    ConstsSpec consts_spec() const;
     PairConsts pair_consts(const double* p) const;
     FinishConsts finish_consts(const double* p, const SetView& set) const;
 };

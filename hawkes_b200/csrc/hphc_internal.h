@@ -1,0 +1,29 @@
+// Library-internal interface between the engine (hphc_engine.cpp) and the
+// device-resident sampler driver (hphc_sampler.cu).  Not part of the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "hphc.h"
+#include "hphc_executor.h"
+#include "hphc_kernels.cuh"
+
+namespace hphc {
+
+// What the device-resident loop needs from an engine after set-up.
+struct EngineLoop {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    Executor* ex = nullptr;
+    ConstsSpec spec{};
+};
+
+// Upload the engine's events if needed and prepare its executor's device
+// loop for K problems on them at params (K x 6).  On failure returns a status
+// and sets *err.
+int engine_loop_setup(hphc_engine* engine, const double* params, int K, EngineLoop* out,
+                      std::string* err);
+
+}  // namespace hphc

@@ -64,6 +64,83 @@ struct FinishConsts {
     int D;
 };
 
+// What param_consts needs besides the parameters: fixed per engine (mode)
+// or per set.
+struct ConstsSpec {
+    int precision;    // HPHC_PRECISION_* (0 = FP64)
+    int D;
+    int variant;      // FP32 variant bits (2 = software exponential)
+    int skip;         // tile-level underflow skip on
+    double ex2Bias;   // mean relative error of ex2.approx (hardware-exponential variant)
+};
+
+// Underflow thresholds (natural-log units) for the tile-pair skip.  FP32:
+// both exponentials return +0 for any argument below -126.5 (log2 units); a
+// true exponent <= -88 is <= -126.96 in log2 units, which the FP32 rounding
+// of the computed exponent (relative ~1e-6) cannot lift above -126.5.  FP64:
+// exp(x) is +0 for x < -745.14; -760 leaves a wide margin.
+constexpr double kSkipF32 = 88.0;
+constexpr double kSkipF64 = 760.0;
+
+// The parameter-dependent constants of one problem: every PairConsts field
+// and every FinishConsts field except T and constant (which depend on the
+// event set only).  Written for host and device alike with products for the
+// integer powers and the correctly rounded sqrt as the only library call, so
+// both give the same bits (the device-resident sampler rewrites them there).
+#ifdef __CUDACC__
+__host__ __device__
+#endif
+inline void param_consts(const double* p, const ConstsSpec& s, PairConsts& c, FinishConsts& f) {
+    const double kLog2eC = 1.44269504088896340735992468100189214;
+    const double kTwoPiC = 6.28318530717958647692528676655900577;
+    const double kInvSqrt2PiC = 0.398942280401432677939946059934;
+    const double sigma = p[0], a = p[1], b = p[2], omega = p[3];
+    const bool fp32 = s.precision != 0;
+    c.cA = -0.5 * a * a;
+    c.cB = -0.5 * b * b;
+    c.cS = -0.5 * sigma * sigma;
+    c.cW = -omega;
+    const double recScale = sqrt(0.5 * kLog2eC);  // record scale per unit precision
+    const double sX = fabs(a) * recScale, sT = fabs(b) * recScale;
+    if (fp32) {
+        const double kS = -(sigma * sigma) / (a * a), kW = -omega * kLog2eC / sT;
+        c.fSh = (float)kS;
+        c.fSl = (float)(kS - (double)c.fSh);
+        c.fWh = (float)kW;
+        c.fWl = (float)(kW - (double)c.fWh);
+    } else {
+        c.fSh = c.fSl = c.fWh = c.fWl = 0.0f;
+    }
+    const double thr = fp32 ? kSkipF32 : kSkipF64;
+    c.skipB = (s.skip && c.cB < 0.0 && c.cA <= 0.0) ? thr : -1.0;
+    c.skipS = (s.skip && c.cW < 0.0 && c.cS <= 0.0) ? thr : -1.0;
+
+    double aD = 1.0, sigmaD = 1.0;
+    for (int k = 0; k < s.D; ++k) {
+        aD *= a;
+        sigmaD *= sigma;
+    }
+    f.sigma = sigma;
+    f.a = a;
+    f.b = b;
+    f.omega = omega;
+    f.theta = p[4];
+    f.mu0 = p[5];
+    f.bgScale = aD * b / kTwoPiC;
+    f.seScale = omega * sigmaD * kInvSqrt2PiC;
+    f.prefB = f.mu0 * f.bgScale;
+    f.prefS = f.theta * f.seScale;
+    for (int q = 0; q < kNumAcc; ++q) f.accScale[q] = 1.0;
+    if (fp32) {
+        f.accScale[1] = f.accScale[4] = 1.0 / (sX * sX);  // sums of d'^2
+        f.accScale[2] = 1.0 / (sT * sT);                  // sum of dt'^2
+        f.accScale[5] = 1.0 / sT;                         // sum of dt'
+        if (!(s.variant & 2))  // hardware exponential: divide out its mean relative error
+            for (int q = 0; q < kNumAcc; ++q) f.accScale[q] /= 1.0 + s.ex2Bias;
+    }
+    f.D = s.D;
+}
+
 struct SweepGeometry {
     int N;            // events
     int Npad;         // stride of the partials arrays (>= N)

@@ -97,19 +97,23 @@ class Sampler:
     def __exit__(self, *exc):
         self.close()
 
-    def run(self, evaluator, iterations: int, burnIn: int = 0):
+    def run(self, evaluator, iterations: int, burnIn: int = 0, device: bool = False):
         """Run every chain; returns (samples [K, iterations - burnIn, 6],
         targets [K, iterations - burnIn]).
 
         evaluator: a :class:`CudaHawkes` engine (its batched entry point
         evaluates the K proposals in one run) or a callable mapping a K x 6
-        array of parameter vectors to K log-likelihoods."""
+        array of parameter vectors to K log-likelihoods.  device=True (engine
+        only) runs every iteration on the GPU from one captured CUDA graph."""
         M = int(iterations) - int(burnIn)
         samples = np.zeros((self.numChains, max(M, 0), 6))
         targets = np.zeros((self.numChains, max(M, 0)))
         if isinstance(evaluator, CudaHawkes):
-            st = _lib.hphc_sampler_run(self._h, evaluator._h, int(iterations), int(burnIn),
-                                       samples.ctypes.data_as(_dp), targets.ctypes.data_as(_dp))
+            fn = _lib.hphc_sampler_run_device if device else _lib.hphc_sampler_run
+            st = fn(self._h, evaluator._h, int(iterations), int(burnIn),
+                    samples.ctypes.data_as(_dp), targets.ctypes.data_as(_dp))
+        elif device:
+            raise HawkesError(3, "run: device=True needs a CudaHawkes engine")
         else:
             st = self._run_callable(evaluator, iterations, burnIn, samples, targets)
         self._check(st, "run")
@@ -153,7 +157,8 @@ class Sampler:
 
 def sampler(n_iter: int, burnIn: int = 0, locations=None, times=None, radius: float = 2.0,
             params=BASE_PARAMS, latentDimension: int = 2, threads: int = 1, simd: int = 0,
-            gpu: int = 1, single: int = 0, chains: int = 1, seed: int = 0) -> dict:
+            gpu: int = 1, single: int = 0, chains: int = 1, seed: int = 0,
+            on_device: bool = False) -> dict:
     """The reference's ``sampler()`` (R/Untitled.R:254-422) on the CUDA engine.
 
     Returns {"samples": 6 x (n_iter - burnIn) (chains x 6 x ... for
@@ -162,7 +167,9 @@ def sampler(n_iter: int, burnIn: int = 0, locations=None, times=None, radius: fl
     signature compatibility and ignored; ``gpu`` is the device number as in
     ``createEngine``; ``single`` selects the FP32-compensated mode; ``chains``
     runs that many independent chains from ``params`` (each with its own
-    random stream), their proposals evaluated together."""
+    random stream), their proposals evaluated together; ``on_device`` runs the
+    iterations as one replayed CUDA graph (tauX and tauT stay fixed, as in the
+    reference's sampler)."""
     if locations is None:
         raise HawkesError(3, "No locations found.")
     if times is None:
@@ -173,7 +180,7 @@ def sampler(n_iter: int, burnIn: int = 0, locations=None, times=None, radius: fl
     init = np.tile(np.asarray(params, dtype=np.float64).reshape(1, 6), (int(chains), 1))
     with Sampler(init, radius=radius, seed=seed) as s:
         t0 = time.perf_counter()
-        samples, targets = s.run(eng["engine"], n_iter, burnIn)
+        samples, targets = s.run(eng["engine"], n_iter, burnIn, device=on_device)
         elapsed = time.perf_counter() - t0
     eng["engine"].close()
     samples = np.transpose(samples, (0, 2, 1))  # chains x 6 x M, as ParametersSaved

@@ -252,6 +252,18 @@ int hphc_sampler_run(hphc_sampler* sampler, hphc_engine* engine, int iterations,
 int hphc_sampler_run_with(hphc_sampler* sampler, hphc_batch_loglik_fn evaluate, void* user,
                           int iterations, int burnIn, double* samples, double* targets);
 
+/* The same iterations run entirely on the device: the chains live in device
+ * memory and one iteration (proposal kernel, pair sweep, finish, acceptance
+ * kernel) is captured once into a CUDA graph and replayed for every
+ * iteration, with no host work or transfer in between; the samples come back
+ * at the end.  The chains continue from, and return to, the sampler's state.
+ * The sampled set must leave tauXprec and tauTprec fixed (they fix the record
+ * scaling and the work list); otherwise HPHC_ERR_UNSUPPORTED.  Chains match
+ * hphc_sampler_run's except where the device math library rounds log, cos,
+ * erfc, exp or pow differently in the last bit. */
+int hphc_sampler_run_device(hphc_sampler* sampler, hphc_engine* engine, int iterations,
+                            int burnIn, double* samples, double* targets);
+
 /* Current state per chain (each pointer may be null): parameters (numChains x
  * 6), potential (NaN before the first run), radii (numChains x 6), accepted
  * and proposed counts. */
