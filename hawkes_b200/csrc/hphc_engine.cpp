@@ -9,10 +9,16 @@
 // so per-row updateLocations calls (src/benchmark.cpp:167-171) cost a host
 // write each rather than a transfer each.
 //
+// After an evaluation of its own parameters the engine keeps every event's six
+// unit pair sums on the device: a later evaluation at the same parameters
+// after a few single-event moves updates them in O(N) per moved event
+// (incremental path), and one with nothing changed re-runs only the O(N)
+// finish.  storeState / restoreState save and bring back those sums.
+//
 // hphc_multiset holds several independent event sets (uneven sizes) for
 // evaluating each at its own parameter vector in one run.
 //
-// Every evaluation goes through hphc::Executor: one launch per stage for any
+// Every sweep goes through hphc::Executor: one launch per stage for any
 // number of (event set, parameter vector) problems, replayed from a CUDA graph.
 #include <cuda_runtime.h>
 

@@ -217,17 +217,30 @@ int Executor::build_plan(const std::vector<SetView>& sets, const int* setOf, con
             colOff += (size_t)(fp32 ? 3 : 6) * Npad;
         }
         if (fp32) {
-            sp.rec = reinterpret_cast<const void*>(recOff);  // offset, fixed up later
-            PackJob j{};
-            j.loc = s.dLoc;
-            j.times = s.dTimes;
-            j.ranks = s.dRanks;
-            j.rec = reinterpret_cast<float*>(recOff);
-            j.sX = record_scale(prm[1]);
-            j.sT = record_scale(prm[2]);
-            j.N = N;
-            pl.pj.push_back(j);
-            recOff += (size_t)N * S32;
+            // problems on the same set with the same tauX and tauT (sampler
+            // chains, proposals that leave them fixed) share one record copy
+            const double sX = record_scale(prm[1]), sT = record_scale(prm[2]);
+            size_t off = recOff;
+            bool shared = false;
+            for (const PackJob& j : pl.pj)
+                if (j.loc == s.dLoc && j.sX == sX && j.sT == sT) {
+                    off = reinterpret_cast<size_t>(j.rec);
+                    shared = true;
+                    break;
+                }
+            sp.rec = reinterpret_cast<const void*>(off);  // offset, fixed up later
+            if (!shared) {
+                PackJob j{};
+                j.loc = s.dLoc;
+                j.times = s.dTimes;
+                j.ranks = s.dRanks;
+                j.rec = reinterpret_cast<float*>(recOff);
+                j.sX = sX;
+                j.sT = sT;
+                j.N = N;
+                pl.pj.push_back(j);
+                recOff += (size_t)N * S32;
+            }
         } else {
             sp.rec = s.dRecF64;
         }
@@ -449,7 +462,7 @@ int Executor::launch_sequence(int grid) {
     if ((e = cudaMemcpyAsync(dTables_, hStaging_, tablesBytes_, cudaMemcpyHostToDevice, stream_)))
         return cuda_fail(e, "stage tables");
     if (prec == 1) {
-        if ((e = launch_pack_f32_jobs(D_, pl.P, pl.maxN, pj, stream_)))
+        if ((e = launch_pack_f32_jobs(D_, (int)pl.pj.size(), pl.maxN, pj, stream_)))
             return cuda_fail(e, "pack kernel");
         ++launches;
     }
@@ -568,6 +581,7 @@ int Executor::enqueue(const std::vector<SetView>& sets, const int* setOf, const 
     }
     GraphKey key;
     key.P = plan_.P;
+    key.nJobs = (int)plan_.pj.size();
     key.nBlocks = plan_.nBlocks;
     key.maxN = plan_.maxN;
     key.R = R;
@@ -576,7 +590,8 @@ int Executor::enqueue(const std::vector<SetView>& sets, const int* setOf, const 
     key.colNeed = colNeed_;
     key.tables = dTables_;
     key.timing = kernelTiming;
-    const bool same = graphExec_ && key.P == graphKey_.P && key.nBlocks == graphKey_.nBlocks &&
+    const bool same = graphExec_ && key.P == graphKey_.P && key.nJobs == graphKey_.nJobs &&
+                      key.nBlocks == graphKey_.nBlocks &&
                       key.maxN == graphKey_.maxN && key.R == graphKey_.R &&
                       key.grid == graphKey_.grid && key.tablesBytes == graphKey_.tablesBytes &&
                       key.colNeed == graphKey_.colNeed &&
@@ -651,7 +666,7 @@ int Executor::setup_device_loop(const std::vector<SetView>& sets, const int* set
         return cuda_fail(e, "stage tables");
     if (precision_ != HPHC_PRECISION_FP64) {
         char* d = static_cast<char*>(dTables_);
-        if ((e = launch_pack_f32_jobs(D_, plan_.P, plan_.maxN,
+        if ((e = launch_pack_f32_jobs(D_, (int)plan_.pj.size(), plan_.maxN,
                                       reinterpret_cast<const PackJob*>(d + offPJ_), stream_)))
             return cuda_fail(e, "pack kernel");
     }

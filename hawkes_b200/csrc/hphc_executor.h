@@ -3,7 +3,8 @@
 //
 //   stage   what                                          launch
 //   H2D     problem tables, work items, finish tables    one cudaMemcpyAsync from pinned staging
-//   pack    FP32 records scaled per problem (FP32 mode)   pack_f32_jobs_kernel, grid (N, P)
+//   pack    FP32 records scaled per problem (FP32 mode;   pack_f32_jobs_kernel, grid (N, jobs)
+//           one copy per distinct set, tauX, tauT)
 //   sweep   persistent CTAs over the work list            sweep_*_list_kernel
 //   finish  per-event contributions, per-CTA sums        finish_list_kernel
 //   final   per-problem fixed-order totals               final_list_kernel
@@ -147,7 +148,7 @@ private:
     // graph
     cudaGraphExec_t graphExec_ = nullptr;
     struct GraphKey {
-        int P = -1, nBlocks = -1, maxN = -1, R = -1, grid = -1;
+        int P = -1, nJobs = -1, nBlocks = -1, maxN = -1, R = -1, grid = -1;
         size_t tablesBytes = 0, colNeed = 0;
         void* tables = nullptr;
         bool timing = false;
