@@ -19,6 +19,12 @@ pair.  "e2e" repeats the measurement through the public API with host buffers
 (setTimesData / updateLocations / setParameters / getLogLikelihoodAndGradient,
 host->device copies and the result read-back inside the timed region).
 
+--shard: the same N = 100,000 evaluation split across the ranks (strong
+scaling): each rank sweeps its share of the target strips, the shares of the
+per-event unit sums (6 N doubles per rank) are all-gathered over NCCL and
+every rank runs the O(N) finish (hawkes_b200.shard).  The step is timed with
+CUDA events on the engine's stream around sweep, gather and finish.
+
 --impl reference: the reference's own CPU engine (hpHawkes NewHawkes, double,
 "TBB" path over all host cores, compiled from its sources into oracle/_ref) on
 a bounded sample of the same workload; rank 0 alone runs it.
@@ -551,6 +557,117 @@ def ours_arm(args):
     return 0
 
 
+def shard_arm(args):
+    """One likelihood per step, split across the ranks (strong scaling)."""
+    import torch
+
+    import hawkes_b200 as hb
+    from hawkes_b200.shard import ShardedHawkes
+
+    rank, world, local = env_int("RANK", 0), env_int("WORLD_SIZE", 1), env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    ranks = Ranks(world, "nccl", dev)
+    barrier = ranks.barrier
+    w = make_workload("headline", args.n)
+    loc, t, p = w["loc"], w["t"], w["params"]
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+
+    def make(flags):
+        e = hb.CudaHawkes(2, len(t), flags, local)
+        e.setTimesData(t)
+        e.updateLocations(-1, loc)
+        e.setParameters(p)
+        return e, ShardedHawkes(e)
+
+    eng64, sh64 = make(hb.CUDA)
+    res64 = sh64.getLogLikelihoodAndGradient()
+    eng64.close()
+    eng, sh = make(hb.CUDA | hb.COMPENSATED)
+    ext = torch.cuda.ExternalStream(eng.stream, device=dev)
+    eng.setKernelTiming(True)
+    for _ in range(args.warmup):
+        sh.getLogLikelihoodAndGradient()
+    # launches of one step: the share's sweep, the rank-ordered sum, the finish
+    sh.sweep()
+    n_sweep = eng.lastLaunchStats()[0]
+    res = eng.getLogLikelihoodAndGradient()
+    launches = n_sweep + 1 + eng.lastLaunchStats()[0]
+    step_ms, sweep_ms = [], []
+    with ClockSampler() as clocks:
+        barrier()
+        for _ in range(args.steps):
+            with torch.cuda.stream(ext):
+                flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(ext)
+            sh.sweep()
+            sweep_ms.append(eng.kernelTimes()[0])
+            res = eng.getLogLikelihoodAndGradient()
+            b.record(ext)
+            b.synchronize()
+            step_ms.append(a.elapsed_time(b))
+        barrier()
+    ms, sweep_max = ranks.max([statistics.mean(step_ms), statistics.mean(sweep_ms)])
+
+    def e2e_step():
+        eng.setTimesData(t)
+        eng.updateLocations(-1, loc)
+        eng.setParameters(p)
+        return sh.getLogLikelihoodAndGradient()
+
+    for _ in range(args.warmup):
+        e2e_step()
+    barrier()
+    n_e2e = max(1, min(args.steps, 50))
+    t0 = time.perf_counter()
+    for _ in range(n_e2e):
+        e2e_step()
+    e2e_s = ranks.max([(time.perf_counter() - t0) / n_e2e])[0]
+    clock_summary = clocks.summary(None)
+    eng.close()
+    ranks.close()
+    if rank != 0:
+        return 0
+    pairs = w["pairs"]
+    peaks, peak_src = measured_peaks()
+    sm_count = torch.cuda.get_device_properties(local).multi_processor_count
+    max_mhz = float(peaks.get("sm_max_mhz", 1965.0))
+    peak_inst = sm_count * FP32_LANES_PER_SM * max_mhz * 1e6 / 1e12
+    achieved = FP32_PER_PAIR_EVAL * pairs / world / (sweep_max / 1e3) / 1e12
+    out = {
+        "metric": METRIC, "value": pairs / (ms / 1e3), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "f32 pair terms (compensated), f64 reductions", "data": "synthetic",
+        "config": dict({"workload": w["desc"], "precision": "fp32-compensated",
+                        "l2": "flushed before every timed step (256 MiB write, outside the "
+                              "timing)",
+                        "parallelism": f"target strips sharded x{world}, unit sums "
+                                       "all-gathered (NCCL), finish on every rank"},
+                       **w["config"]),
+        "accuracy": {"loglik_rel_vs_fp64": abs(res[0] - res64[0]) / abs(res64[0]),
+                     "grad_rel_vs_fp64": [float(abs(x - y) / abs(y))
+                                          for x, y in zip(res[1], res64[1])]},
+        "roofline": {"bound": "fp32", "kernel": "sweep_f32c_list_kernel (one rank's share)",
+                     "achieved": achieved, "peak": peak_inst, "unit": "Tinst/s",
+                     "frac": achieved / peak_inst, "traffic": None,
+                     "count": f"{FP32_PER_PAIR_EVAL} FP32 instructions per pair-eval x "
+                              f"{pairs:.4g} / {world} pair-evals per rank, over the slowest "
+                              "rank's mean sweep duration",
+                     "peak_source": f"{sm_count} SMs x 128 FP32 lanes x {max_mhz:.0f} MHz "
+                                    f"(sm_max_mhz, {peak_src})",
+                     "sweep_ms": sweep_max},
+        "e2e": {"value": pairs / e2e_s, "unit": UNIT, "h2d_bytes_per_step": w["h2d"],
+                "d2h_bytes_per_step": w["d2h"]},
+        "gpu_launches": launches * args.steps,
+        "clocks": clock_summary,
+    }
+    print(json.dumps(out))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -568,9 +685,14 @@ def main():
     ap.add_argument("--shape", default="",
                     help="fix the sweep shape as R:ITEMS_PER_SM instead of autotuning it "
                          "(e.g. to profile one shape)")
+    ap.add_argument("--shard", action="store_true",
+                    help="split the one N=100k evaluation across the ranks (strong scaling) "
+                         "instead of one replica per rank")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
+    if args.shard:
+        return shard_arm(args)
     return ours_arm(args)
 
 

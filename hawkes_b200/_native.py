@@ -47,6 +47,10 @@ SIGNATURES = {
     "hphc_loglik_grad_fp64_static": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
                                                     ctypes.c_void_p, _c_double_p,
                                                     ctypes.c_void_p, ctypes.c_void_p]),
+    "hphc_sweep_shard": (ctypes.c_int, [_handle, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                        ctypes.c_size_t]),
+    "hphc_set_unit_sums": (ctypes.c_int, [_handle, ctypes.c_void_p, ctypes.c_int,
+                                          ctypes.c_size_t]),
     "hphc_set_kernel_timing": (ctypes.c_int, [_handle, ctypes.c_int]),
     "hphc_set_sweep_shape": (ctypes.c_int, [_handle, ctypes.c_int, ctypes.c_int]),
     "hphc_get_sweep_shape": (ctypes.c_int, [_handle, _c_int_p, _c_int_p]),

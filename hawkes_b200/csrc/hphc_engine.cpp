@@ -142,6 +142,7 @@ struct Mode {
     int variant = 2;  // FP32 variant bits: 1 = coordinate lo parts, 2 = software exponential
     bool underflowSkip = true;
     bool symmetric = true;  // each background pair evaluated once for both events
+    bool fastTail = true;   // far-tail background tile pairs on the hardware exponential
 };
 
 Mode mode_from_flags(long fl) {
@@ -152,6 +153,7 @@ Mode mode_from_flags(long fl) {
     m.variant = ((fl & HPHC_FLAG_FP32_SPACE_HILO) ? 1 : 0) |
                 ((fl & HPHC_FLAG_FP32_FAST_EXP) ? 0 : 2);
     m.symmetric = !(fl & HPHC_FLAG_ORDERED);
+    m.fastTail = !(fl & HPHC_FLAG_NO_FAST_TAIL);
     return m;
 }
 
@@ -322,6 +324,7 @@ struct Runtime {
         const int st = ex.init(D, mode.precision, mode.variant, mode.underflowSkip, device, stream,
                                ex2Bias);
         ex.symmetric = mode.symmetric;
+        ex.fastTail = mode.fastTail;
         if (st) err = ex.error;
         return st;
     }
@@ -396,6 +399,11 @@ struct hphc_engine {
     int lastPath = HPHC_PATH_SWEEP;
     double lastIncTerms = 0.0;  // pair terms of the last incremental evaluation
 
+    // Sharded evaluation: the last sweep_shard ran at shardParams on the
+    // current events (cleared when the events change).
+    bool shardValid = false;
+    double shardParams[6] = {0, 0, 0, 0, 0, 0};
+
     void clear_moved() {
         for (int k : moved) movedSlot[k] = -1;
         moved.clear();
@@ -404,6 +412,7 @@ struct hphc_engine {
 
     void invalidate_sums() {
         sumsValid = false;
+        shardValid = false;
         clear_moved();
     }
 
@@ -567,6 +576,59 @@ struct hphc_engine {
         if (grad)
             for (int k = 0; k < 6; ++k) grad[k] = hIncOut.p[1 + k];
         lastPath = hadMoves ? HPHC_PATH_INCREMENTAL : HPHC_PATH_KEPT_SUMS;
+        return HPHC_OK;
+    }
+
+    // Rank `rank` of `world`: this rank's share of the unit pair sums at the
+    // current parameters into dPart ([6][N], natural units).
+    int sweep_shard(int rank, int world, double* dPart) {
+        lastLaunches = 0;
+        lastPath = HPHC_PATH_SWEEP;
+        shardValid = false;
+        if (!moved.empty() || recStale) dirty = true;
+        int st = upload_if_dirty();
+        if (st) return st;
+        std::vector<SetView> sets{set.view()};
+        const int setOf = 0;
+        rt.ex.sumsOut = dPart;
+        rt.ex.shardRank = rank;
+        rt.ex.shardWorld = world;
+        st = rt.ex.enqueue(sets, &setOf, params, 1, nullptr);
+        if (st == HPHC_OK) {
+            lastLaunches += rt.ex.lastLaunches;
+            hOut.resize(8);
+            st = rt.ex.wait(hOut.data());  // its log-likelihood is of a share: not used
+        }
+        rt.ex.sumsOut = nullptr;
+        rt.ex.shardRank = 0;
+        rt.ex.shardWorld = 1;
+        if (st) return fmt(lastError, st, "%s", rt.ex.error.c_str());
+        shardValid = true;
+        std::memcpy(shardParams, params, sizeof shardParams);
+        return HPHC_OK;
+    }
+
+    // The sums of nParts shares (rank order) become the kept sums at the
+    // current parameters.
+    int set_unit_sums(const double* dParts, int nParts) {
+        if (!incremental)
+            return fail(HPHC_ERR_UNSUPPORTED,
+                        "unit sums: the engine keeps no sums (HPHC_FLAG_NO_INCREMENTAL)");
+        if (!shardValid || dirty || !moved.empty() ||
+            std::memcmp(params, shardParams, sizeof shardParams) != 0)
+            return fail(HPHC_ERR_BAD_ARGUMENT,
+                        "unit sums: events or parameters changed since this engine's "
+                        "hphc_sweep_shard");
+        const size_t n = (size_t)kNumAcc * N;
+        cudaError_t e = launch_sum_parts(dParts, nParts, n, dSums.p, rt.ex.num_sms(), rt.stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(rt.stream);
+        if (e != cudaSuccess) {
+            invalidate_sums();
+            return cuda_status(lastError, e, "sum of the shares");
+        }
+        pendingSums = false;
+        sumsValid = true;
+        std::memcpy(sumsParams, params, sizeof sumsParams);
         return HPHC_OK;
     }
 
@@ -900,6 +962,47 @@ int hphc_read_results(hphc_engine* e, double* loglik, double* gradient, size_t l
     if (gradient)
         for (int k = 0; k < 6; ++k) gradient[k] = e->hOut[1 + k];
     return HPHC_OK;
+}
+
+// A device pointer on the engine's device (or managed memory).
+static bool device_pointer_on(const void* p, int device) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return (a.type == cudaMemoryTypeDevice && a.device == device) ||
+           a.type == cudaMemoryTypeManaged;
+}
+
+int hphc_sweep_shard(hphc_engine* e, int rank, int world, double* devicePart, size_t length) {
+    if (!e) return HPHC_ERR_INVALID_HANDLE;
+    if (world < 1 || rank < 0 || rank >= world)
+        return e->fail(HPHC_ERR_BAD_ARGUMENT, "shard: rank %d of world %d", rank, world);
+    if (length != (size_t)kNumAcc * e->N)
+        return e->fail(HPHC_ERR_BAD_LENGTH, "shard: length %zu != 6 * locationCount = %zu",
+                       length, (size_t)kNumAcc * e->N);
+    DeviceGuard g(e->rt.device);
+    if (!g.ok) return e->fail(HPHC_ERR_CUDA, "cannot select device %d", e->rt.device);
+    if (!devicePart || !device_pointer_on(devicePart, e->rt.device))
+        return e->fail(HPHC_ERR_BAD_ARGUMENT, "shard: output is not device memory of device %d",
+                       e->rt.device);
+    return e->sweep_shard(rank, world, devicePart);
+}
+
+int hphc_set_unit_sums(hphc_engine* e, const double* deviceParts, int numParts, size_t length) {
+    if (!e) return HPHC_ERR_INVALID_HANDLE;
+    if (numParts < 1) return e->fail(HPHC_ERR_BAD_ARGUMENT, "unit sums: %d parts", numParts);
+    if (length != (size_t)numParts * kNumAcc * e->N)
+        return e->fail(HPHC_ERR_BAD_LENGTH,
+                       "unit sums: length %zu != parts * 6 * locationCount = %zu", length,
+                       (size_t)numParts * kNumAcc * e->N);
+    DeviceGuard g(e->rt.device);
+    if (!g.ok) return e->fail(HPHC_ERR_CUDA, "cannot select device %d", e->rt.device);
+    if (!deviceParts || !device_pointer_on(deviceParts, e->rt.device))
+        return e->fail(HPHC_ERR_BAD_ARGUMENT,
+                       "unit sums: input is not device memory of device %d", e->rt.device);
+    return e->set_unit_sums(deviceParts, numParts);
 }
 
 int hphc_get_last_evaluation_path(hphc_engine* e, int* path) {

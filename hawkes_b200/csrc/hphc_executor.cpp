@@ -112,6 +112,7 @@ ConstsSpec Executor::consts_spec() const {
     s.variant = variant_;
     s.skip = skip_ ? 1 : 0;
     s.ex2Bias = ex2Bias_;
+    s.fastTail = fastTail ? 1 : 0;
     return s;
 }
 
@@ -159,7 +160,9 @@ int Executor::build_plan(const std::vector<SetView>& sets, const int* setOf, con
         const SetView& s = sets[setOf[p]];
         totalStrips += (s.N + stripEvents - 1) / stripEvents;
     }
-    const int target = numSMs_ * items;
+    // a shard keeps about 1/shardWorld of the items: cut finer chunks so that
+    // each rank still has `items` per SM
+    const int target = numSMs_ * items * std::max(1, shardWorld);
     const int nChunksTarget = std::max(1, (int)std::ceil(target / std::max(1.0, totalStrips)));
 
     size_t recOff = 0, partOff = 0, colOff = 0;
@@ -339,6 +342,33 @@ int Executor::build_plan(const std::vector<SetView>& sets, const int* setOf, con
         blockBase += fp.nBlocks;
     }
     pl.nBlocks = blockBase;
+    if (shardWorld > 1) {
+        // Longest-processing-time assignment of whole strips to ranks by
+        // their tile counts; ties go to the lower strip and the lower rank,
+        // so every rank derives the same assignment from the same plan.
+        const size_t nS = pl.stripChunks.size();
+        std::vector<double> cost(nS, 0.0);
+        for (const WorkItem& w : pl.items) cost[chunkBase[w.problem] + w.strip] += w.jt1 - w.jt0;
+        std::vector<int> order(nS);
+        for (size_t k = 0; k < nS; ++k) order[k] = (int)k;
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int x, int y) { return cost[x] > cost[y]; });
+        std::vector<double> load(shardWorld, 0.0);
+        std::vector<char> owned(nS, 0);
+        for (int k : order) {
+            int best = 0;
+            for (int r = 1; r < shardWorld; ++r)
+                if (load[r] < load[best]) best = r;
+            load[best] += cost[k];
+            owned[k] = best == shardRank;
+        }
+        size_t kept = 0;
+        for (const WorkItem& w : pl.items)
+            if (owned[chunkBase[w.problem] + w.strip]) pl.items[kept++] = w;
+        pl.items.resize(kept);
+        for (size_t k = 0; k < nS; ++k)
+            if (!owned[k]) pl.stripChunks[k] = 0;
+    }
     std::stable_sort(pl.items.begin(), pl.items.end(), [](const WorkItem& x, const WorkItem& y) {
         return (x.jt1 - x.jt0) > (y.jt1 - y.jt0);
     });
@@ -492,6 +522,7 @@ int Executor::autotune(const std::vector<SetView>& sets, const int* setOf, const
                        int P, double* dProbs) {
     double pairs = 0.0;
     for (int p = 0; p < P; ++p) pairs += (double)sets[setOf[p]].N * sets[setOf[p]].N;
+    pairs /= std::max(1, shardWorld);  // work of this rank
     const auto key = std::make_tuple(D_, precision_, variant_ | (symmetric ? 16 : 0),
                                      log2_bucket(pairs), log2_bucket(P));
     {

@@ -80,6 +80,7 @@ public:
     SweepProblem* device_sweep_problems() const;
     FinishProblem* device_finish_problems() const;
     const double* device_results() const { return dOut_; }
+    int num_sms() const { return numSMs_; }
 
     // Pair terms the last run's sweep accounted for (replays the tile
     // decisions): background terms (both orders of a symmetric pair),
@@ -93,6 +94,14 @@ public:
     bool useGraph = true;
     bool kernelTiming = false;
     bool symmetric = false;  // symmetric background sweep (set before the first enqueue)
+    bool fastTail = true;    // FP32 polynomial mode: far-tail tile pairs use ex2.approx
+    // Sharded sweep: with shardWorld > 1 the plan keeps only the target
+    // strips assigned to shardRank (whole strips, balanced by their tile
+    // counts; every rank computes the same assignment), and the finish takes
+    // the other strips' row sums as zero.  The unit sums written to sumsOut
+    // are then this rank's share; the shares of all ranks add up to the sums
+    // of the unsharded sweep.
+    int shardRank = 0, shardWorld = 1;
     double* sumsOut = nullptr;  // if set, problem 0's unit pair sums ([6][N], natural units)
     float lastSweepMs = 0.f, lastFinishMs = 0.f, lastStepMs = 0.f;
     bool timedValid = false;

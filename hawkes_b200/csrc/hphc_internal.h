@@ -26,4 +26,9 @@ struct EngineLoop {
 int engine_loop_setup(hphc_engine* engine, const double* params, int K, EngineLoop* out,
                       std::string* err);
 
+// out[k] = parts[k] + parts[n + k] + ... + parts[(nParts - 1) n + k], added in
+// that order (hphc_shard.cu).
+cudaError_t launch_sum_parts(const double* parts, int nParts, size_t n, double* out, int numSMs,
+                             cudaStream_t s);
+
 }  // namespace hphc

@@ -111,6 +111,7 @@ tile_bounds_kernel(int N, const double* __restrict__ times, double* __restrict__
 
 struct TileMode {
     bool doB, doS, allCausal;
+    bool fastB;  // every background term of the pair is in the far tail (FP32)
 };
 
 // dt = t_i - t_j over the tile pair lies in [tminI - tmaxJ, tmaxI - tminJ].
@@ -123,6 +124,7 @@ __device__ __forceinline__ TileMode tile_mode(double tminI, double tmaxI, double
     m.allCausal = dtLo > 0.0;
     const bool anyCausal = dtHi > 0.0;
     m.doS = anyCausal && !(c.skipS >= 0.0 && m.allCausal && -c.cW * dtLo >= c.skipS);
+    m.fastB = c.fastB >= 0.0 && -c.cB * minAbs * minAbs >= c.fastB;
     return m;
 }
 
@@ -493,8 +495,9 @@ __device__ __forceinline__ float2 exp2_poly_neg2(float2 s) {
     return mul2(p, make_float2(ex2_ftz(-m.x), ex2_ftz(-m.y)));
 }
 
-// Background unit terms 2^-(d2 + t2).  The hardware exponential's mean
-// relative error is divided out of the sums in the FP64 finish.
+// Background unit terms 2^-(d2 + t2).  In the hardware-exponential variant its
+// mean relative error is divided out of the sums in the FP64 finish; far-tail
+// terms of the polynomial variant (at most 2^-12 each) keep it.
 template <int V>
 __device__ __forceinline__ float2 background2(float2 s) {
     if (V & kPolyExp) return exp2_poly_neg2(s);
@@ -554,7 +557,7 @@ __device__ __forceinline__ void geometry2(const StagedTile<D>& t, int p, const R
 
 // Row-order pass over column pairs [p0, p1) of the staged tile (broadcast
 // reads shared by the R rows).
-template <int D, int R, int V, bool DO_B, bool DO_S, bool MASK>
+template <int D, int R, int V, int VB, bool DO_B, bool DO_S, bool MASK>
 __device__ __forceinline__ void body_f32(const StagedTile<D>& t, int p0, int p1,
                                          const Rows2<D, R>& w, const PairConsts& c,
                                          float2 (&a)[R][kNumAcc]) {
@@ -567,7 +570,7 @@ __device__ __forceinline__ void body_f32(const StagedTile<D>& t, int p0, int p1,
             geometry2<D, R, V>(t, p, w, r, d2, dt);
             if (DO_B) {
                 const float2 t2 = mul2(dt, dt);
-                const float2 B = background2<V>(add2(d2, t2));
+                const float2 B = background2<VB>(add2(d2, t2));
                 a[r][0] = add2(a[r][0], B);
                 a[r][1] = fma2(B, d2, a[r][1]);
                 a[r][2] = fma2(B, t2, a[r][2]);
@@ -599,14 +602,14 @@ __device__ __forceinline__ void flush_rows(const float2 (&a)[R][kNumAcc],
         for (int q = 0; q < kNumAcc; ++q) acc[r][q] += (double)(a[r][q].x + a[r][q].y);
 }
 
-template <int D, int R, int V, bool DO_B, bool DO_S, bool MASK>
+template <int D, int R, int V, int VB, bool DO_B, bool DO_S, bool MASK>
 __device__ __forceinline__ void tile_f32(const StagedTile<D>& t, int nj, const Rows2<D, R>& w,
                                          const PairConsts& c, double (&acc)[R][kNumAcc]) {
     const int nPairs = (nj + 1) / 2;
     for (int p0 = 0; p0 < nPairs; p0 += kFlush / 2) {
         float2 a[R][kNumAcc];
         zero_rows<R>(a);
-        body_f32<D, R, V, DO_B, DO_S, MASK>(t, p0, min(p0 + kFlush / 2, nPairs), w, c, a);
+        body_f32<D, R, V, VB, DO_B, DO_S, MASK>(t, p0, min(p0 + kFlush / 2, nPairs), w, c, a);
         flush_rows<R>(a, acc);
     }
 }
@@ -646,7 +649,7 @@ __device__ __forceinline__ float sym_exchange(const float2 (&cp)[kSymGroup / 2],
     return x;
 }
 
-template <int D, int R, int V, bool DO_S, bool MASK>
+template <int D, int R, int V, int VB, bool DO_S, bool MASK>
 __device__ __forceinline__ void sym_group_f32(const StagedTile<D>& t, int g, int q,
                                               const Rows2<D, R>& w, const PairConsts& c,
                                               float2 (&a)[R][kNumAcc],
@@ -660,7 +663,7 @@ __device__ __forceinline__ void sym_group_f32(const StagedTile<D>& t, int g, int
             float2 d2, dt;
             geometry2<D, R, V>(t, p, w, r, d2, dt);
             const float2 t2 = mul2(dt, dt);
-            const float2 B = background2<V>(add2(d2, t2));
+            const float2 B = background2<VB>(add2(d2, t2));
             a[r][0] = add2(a[r][0], B);
             a[r][1] = fma2(B, d2, a[r][1]);
             a[r][2] = fma2(B, t2, a[r][2]);
@@ -685,7 +688,7 @@ __device__ __forceinline__ void sym_group_f32(const StagedTile<D>& t, int g, int
 
 // One full tile J (kTile columns, all real events) before the strip.
 // sCol: [kSweepThreads / 32][3][kTile] floats of shared memory.
-template <int D, int R, int V, bool DO_S, bool MASK>
+template <int D, int R, int V, int VB, bool DO_S, bool MASK>
 __device__ __forceinline__ void tile_sym_f32(const StagedTile<D>& t, const Rows2<D, R>& w,
                                              const PairConsts& c, double (&acc)[R][kNumAcc],
                                              float* __restrict__ sCol,
@@ -703,7 +706,7 @@ __device__ __forceinline__ void tile_sym_f32(const StagedTile<D>& t, const Rows2
 #pragma unroll 1
         for (int g = jb; g < jb + kFlush; g += kSymGroup) {
             float2 cp[3][kSymGroup / 2];
-            sym_group_f32<D, R, V, DO_S, MASK>(t, g, q, w, c, a, cp);
+            sym_group_f32<D, R, V, VB, DO_S, MASK>(t, g, q, w, c, a, cp);
             const float c0 = sym_exchange(cp[0], hi);
             const float c1 = sym_exchange(cp[1], hi);
             const float c2 = sym_exchange(cp[2], hi);
@@ -810,26 +813,41 @@ __device__ __forceinline__ void f32c_item(const float* __restrict__ rec,
             st.rank[tid] = INT_MAX;
         }
         __syncthreads();
+        // Far-tail tile pairs take their background terms from the hardware
+        // exponential.  The choice depends on the background magnitude alone,
+        // so the underflow skip (which may drop the pair's self-excitation
+        // terms) never changes it.  A far-tail pair has min|dt| > 0: its j
+        // events are all earlier than its i events or all later, so it needs
+        // no causality mask.
+        constexpr int VF = V & ~kPolyExp;
         if (sym && m.doB && jt < ts0) {
             // jt < ts0 <= nTiles - 1: a full tile
-            if (!m.doS)
-                tile_sym_f32<D, R, V, false, false>(st, w, c, acc, sCol, colAcc, Npad, j0);
+            if (m.fastB && !m.doS)
+                tile_sym_f32<D, R, V, VF, false, false>(st, w, c, acc, sCol, colAcc, Npad, j0);
+            else if (m.fastB)
+                tile_sym_f32<D, R, V, VF, true, false>(st, w, c, acc, sCol, colAcc, Npad, j0);
+            else if (!m.doS)
+                tile_sym_f32<D, R, V, V, false, false>(st, w, c, acc, sCol, colAcc, Npad, j0);
             else if (m.allCausal)
-                tile_sym_f32<D, R, V, true, false>(st, w, c, acc, sCol, colAcc, Npad, j0);
+                tile_sym_f32<D, R, V, V, true, false>(st, w, c, acc, sCol, colAcc, Npad, j0);
             else
-                tile_sym_f32<D, R, V, true, true>(st, w, c, acc, sCol, colAcc, Npad, j0);
+                tile_sym_f32<D, R, V, V, true, true>(st, w, c, acc, sCol, colAcc, Npad, j0);
         } else if (m.doB) {
-            if (!m.doS)
-                tile_f32<D, R, V, true, false, false>(st, nj, w, c, acc);
+            if (m.fastB && !m.doS)
+                tile_f32<D, R, V, VF, true, false, false>(st, nj, w, c, acc);
+            else if (m.fastB)
+                tile_f32<D, R, V, VF, true, true, false>(st, nj, w, c, acc);
+            else if (!m.doS)
+                tile_f32<D, R, V, V, true, false, false>(st, nj, w, c, acc);
             else if (m.allCausal)
-                tile_f32<D, R, V, true, true, false>(st, nj, w, c, acc);
+                tile_f32<D, R, V, V, true, true, false>(st, nj, w, c, acc);
             else
-                tile_f32<D, R, V, true, true, true>(st, nj, w, c, acc);
+                tile_f32<D, R, V, V, true, true, true>(st, nj, w, c, acc);
         } else {
             if (m.allCausal)
-                tile_f32<D, R, V, false, true, false>(st, nj, w, c, acc);
+                tile_f32<D, R, V, V, false, true, false>(st, nj, w, c, acc);
             else
-                tile_f32<D, R, V, false, true, true>(st, nj, w, c, acc);
+                tile_f32<D, R, V, V, false, true, true>(st, nj, w, c, acc);
         }
     }
 #pragma unroll

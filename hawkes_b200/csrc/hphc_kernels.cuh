@@ -47,6 +47,10 @@ struct PairConsts {
     // in it is exactly zero in the working precision: cA <= 0, cB < 0 and
     // -cB * min|dt|^2 >= skipB.  Likewise for S with -cW * min(dt) >= skipS.
     double skipB, skipS;                   // natural-log thresholds; < 0 disables
+    // FP32 mode: a tile pair whose background terms are all below
+    // exp(-fastB) (natural log; < 0 disables) takes them from the hardware
+    // exponential (see kFastTailLog2).
+    double fastB;
 };
 
 // Constants of the per-event finish (all FP64).
@@ -72,7 +76,17 @@ struct ConstsSpec {
     int variant;      // FP32 variant bits (2 = software exponential)
     int skip;         // tile-level underflow skip on
     double ex2Bias;   // mean relative error of ex2.approx (hardware-exponential variant)
+    int fastTail;     // FP32 software-exponential variant: far tile pairs use the hardware one
 };
+
+// Far background tail of the FP32 software-exponential mode.  A tile pair
+// whose background terms are all at most 2^-kFastTailLog2 of an event's own
+// term (B_ii = 1 unit) evaluates them with ex2.approx instead of the
+// polynomial.  Such terms lie beyond 3.46 scale units of the time Gaussian
+// (4.1 of its standard deviations), so they carry under 5e-4 of any
+// event's unit sums even weighted by dt'^2, and the hardware exponential's
+// relative error (< 1e-7) moves those sums by under ~5e-11.
+constexpr double kFastTailLog2 = 12.0;
 
 // Underflow thresholds (natural-log units) for the tile-pair skip.  FP32:
 // both exponentials return +0 for any argument below -126.5 (log2 units); a
@@ -114,6 +128,10 @@ inline void param_consts(const double* p, const ConstsSpec& s, PairConsts& c, Fi
     const double thr = fp32 ? kSkipF32 : kSkipF64;
     c.skipB = (s.skip && c.cB < 0.0 && c.cA <= 0.0) ? thr : -1.0;
     c.skipS = (s.skip && c.cW < 0.0 && c.cS <= 0.0) ? thr : -1.0;
+    const double kLn2 = 0.693147180559945309417232121458176568;
+    c.fastB = (fp32 && s.fastTail && (s.variant & 2) && c.cB < 0.0 && c.cA <= 0.0)
+                  ? kFastTailLog2 * kLn2
+                  : -1.0;
 
     double aD = 1.0, sigmaD = 1.0;
     for (int k = 0; k < s.D; ++k) {

@@ -49,6 +49,7 @@ FP32_SPACE_HILO = 1 << 12
 ORDERED = 1 << 13       # both orders of every background pair, either precision
 FP32_ORDERED = ORDERED  # earlier name of the same bit
 NO_INCREMENTAL = 1 << 14
+NO_FAST_TAIL = 1 << 15  # FP32-compensated: polynomial exponential for the far tail too
 
 # How an evaluation was computed (CudaHawkes.lastEvaluationPath).
 PATH_SWEEP = 0
@@ -89,6 +90,7 @@ class CudaHawkes:
         self.embeddingDimension = int(embeddingDimension)
         self.locationCount = int(locationCount)
         self.flags = int(flags)
+        self.device = int(device)
 
     # -- plumbing -------------------------------------------------------------
     def _check(self, st: int, what: str) -> None:
@@ -249,6 +251,24 @@ class CudaHawkes:
         v = ctypes.c_double()
         self._check(_lib.hphc_get_last_launch_evals(self._h, ctypes.byref(v)), "lastLaunchEvals")
         return v.value
+
+    # -- sharded evaluation (hawkes_b200.shard) --------------------------------
+    def sweepShard(self, rank: int, world: int, devicePart: int) -> None:
+        """Rank `rank` of `world`: write this rank's share of every event's six
+        unit pair sums at the current parameters to the device buffer at
+        address devicePart (6 N doubles on the engine's device)."""
+        self._check(_lib.hphc_sweep_shard(self._h, int(rank), int(world),
+                                          ctypes.c_void_p(int(devicePart)),
+                                          6 * self.locationCount), "sweepShard")
+
+    def setUnitSums(self, deviceParts: int, numParts: int) -> None:
+        """Add numParts shares (back to back at device address deviceParts,
+        share r from rank r) in rank order and keep them as the sums at the
+        current parameters; the next evaluation runs only the O(N) finish."""
+        self._check(_lib.hphc_set_unit_sums(self._h, ctypes.c_void_p(int(deviceParts)),
+                                            int(numParts),
+                                            int(numParts) * 6 * self.locationCount),
+                    "setUnitSums")
 
     @property
     def lastEvaluationPath(self) -> int:

@@ -78,6 +78,11 @@ extern "C" {
                                                 an evaluation at unchanged parameters after
                                                 a few single-event updateLocations calls
                                                 updates the kept per-event sums in O(N)) */
+#define HPHC_FLAG_NO_FAST_TAIL (1L << 15)    /* FP32-compensated mode: the polynomial
+                                                exponential for every pair term (by default
+                                                tile pairs whose background terms are all
+                                                below 2^-12 of an event's own term, and that
+                                                hold no self-excitation term, use ex2.approx) */
 
 /* How the last evaluation was computed (hphc_get_last_evaluation_path). */
 #define HPHC_PATH_SWEEP 0        /* the O(N^2) pair sweep                             */
@@ -296,6 +301,32 @@ int hphc_sampler_get_state(const hphc_sampler* sampler, double* params, double* 
 int hphc_loglik_grad_fp64_static(int embeddingDimension, int locationCount,
                                  const double* deviceLocations, const double* deviceTimes,
                                  const double* params, double* deviceOut, void* stream);
+
+/* ---- sharded evaluation across GPUs ---------------------------------------
+ * No reference counterpart (the reference evaluates on one device).  One
+ * engine per GPU, every engine holding all events and the same parameters.
+ * Each rank sweeps a disjoint set of target strips (whole strips, assigned
+ * by the same deterministic balance on every rank) and writes its share of
+ * every event's six unit pair sums; the shares of ranks 0..world-1 add up to
+ * the sums of one unsharded sweep.  The caller moves the shares between GPUs
+ * (one all-gather of 6 N doubles per rank, e.g. NCCL), then gives every rank
+ * all of them: the engine adds them in rank order, so all ranks then hold the
+ * same sums, and its next getSumOfLikContribs / gradient /
+ * getProbsSelfExcite at those parameters runs only the O(N) finish
+ * (HPHC_PATH_KEPT_SUMS).  Needs the kept sums (no HPHC_FLAG_NO_INCREMENTAL).
+ *
+ * hphc_sweep_shard: rank's share into devicePart, device memory of the
+ * engine's device holding length = 6 N doubles ([6][N], natural units).
+ * Synchronous. */
+int hphc_sweep_shard(hphc_engine* engine, int rank, int world, double* devicePart,
+                     size_t length);
+
+/* deviceParts: numParts shares back to back (length = numParts * 6 N doubles,
+ * device memory of the engine's device), share r from rank r.  Fails with
+ * HPHC_ERR_BAD_ARGUMENT if the events or parameters changed since this
+ * engine's own hphc_sweep_shard. */
+int hphc_set_unit_sums(hphc_engine* engine, const double* deviceParts, int numParts,
+                       size_t length);
 
 /* ---- introspection and device-resident timing --------------------------- */
 
