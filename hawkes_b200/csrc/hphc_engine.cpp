@@ -473,8 +473,15 @@ struct hphc_engine {
         hIncOut.release();
     }
 
+    int faultUploads = 0;  // injected upload failures still to deliver
+
     int upload_if_dirty() {
         if (!dirty) return HPHC_OK;
+        NvtxRange range("hphc upload");
+        if (faultUploads > 0) {
+            --faultUploads;
+            return cuda_status(lastError, cudaErrorMemoryAllocation, "upload (injected)");
+        }
         const cudaError_t e = set.upload(hLoc[curLoc].p, rt.mode.precision, rt.stream,
                                          &lastLaunches);
         if (e != cudaSuccess) return cuda_status(lastError, e, "upload");
@@ -485,6 +492,7 @@ struct hphc_engine {
 
     // Enqueue K parameter vectors on this engine's events (full sweep).
     int enqueue(const double* p, int K, bool wantProbs) {
+        NvtxRange range("hphc sweep enqueue");
         lastLaunches = 0;
         lastPath = HPHC_PATH_SWEEP;
         // moved events are only on the host, and after incremental row uploads
@@ -535,6 +543,7 @@ struct hphc_engine {
     // O(N) evaluation from the kept sums: upload and apply each moved event,
     // then the per-event finish.
     int evaluate_incremental(const double* p, double* loglik, double* grad, double* probs) {
+        NvtxRange range("hphc kept-sums finish");
         lastLaunches = 0;
         const bool hadMoves = !moved.empty();
         const bool wasDirty = dirty;
@@ -582,6 +591,7 @@ struct hphc_engine {
     // Rank `rank` of `world`: this rank's share of the unit pair sums at the
     // current parameters into dPart ([6][N], natural units).
     int sweep_shard(int rank, int world, double* dPart) {
+        NvtxRange range("hphc sweep shard");
         lastLaunches = 0;
         lastPath = HPHC_PATH_SWEEP;
         shardValid = false;
@@ -633,6 +643,7 @@ struct hphc_engine {
     }
 
     int evaluate(const double* p, double* loglik, double* grad, double* probs) {
+        NvtxRange range("hphc evaluate");
         DeviceGuard g(rt.device);
         if (!g.ok) return fail(HPHC_ERR_CUDA, "cannot select device %d", rt.device);
         if (can_update(p)) return evaluate_incremental(p, loglik, grad, probs);
@@ -1005,6 +1016,23 @@ int hphc_set_unit_sums(hphc_engine* e, const double* deviceParts, int numParts, 
     return e->set_unit_sums(deviceParts, numParts);
 }
 
+int hphc_inject_fault(hphc_engine* e, int stage, int count) {
+    if (!e) return HPHC_ERR_INVALID_HANDLE;
+    if (count < 0 || (count > 0 && (stage < HPHC_FAULT_UPLOAD || stage > HPHC_FAULT_WAIT)))
+        return e->fail(HPHC_ERR_BAD_ARGUMENT, "fault injection: stage %d, count %d", stage, count);
+    e->faultUploads = 0;
+    e->rt.ex.faultStage = 0;
+    e->rt.ex.faultCount = 0;
+    if (count == 0) return HPHC_OK;
+    if (stage == HPHC_FAULT_UPLOAD) {
+        e->faultUploads = count;
+    } else {
+        e->rt.ex.faultStage = stage;
+        e->rt.ex.faultCount = count;
+    }
+    return HPHC_OK;
+}
+
 int hphc_get_last_evaluation_path(hphc_engine* e, int* path) {
     if (!e) return HPHC_ERR_INVALID_HANDLE;
     if (!path) return e->fail(HPHC_ERR_BAD_ARGUMENT, "null output");
@@ -1150,6 +1178,7 @@ int hphc_multiset_log_likelihood_and_gradient(hphc_multiset* m, const double* pa
         if (!m->ready[s]) return fmt(m->lastError, HPHC_ERR_NOT_READY, "set %d has no data", s);
     DeviceGuard g(m->rt.device);
     if (!g.ok) return fmt(m->lastError, HPHC_ERR_CUDA, "cannot select device %d", m->rt.device);
+    NvtxRange range("hphc multiset evaluate");
     m->lastLaunches = 0;
     std::vector<SetView> views(m->S);
     for (int s = 0; s < m->S; ++s) {

@@ -3,10 +3,14 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <string>
 #include <tuple>
+#include <vector>
 
 #include "hphc.h"
 
@@ -37,10 +41,112 @@ int f32_stride(int D) {
     return (2 * (D + 1) + 1 + 3) / 4 * 4;
 }
 
-// Autotuned sweep shapes per process: (D, precision, variant, log2 of the
+// Autotuned sweep shapes per process: (D, precision, mode bits, log2 of the
 // pair count, log2 of the problem count) -> (R, items per SM).
+using TuneKey = std::tuple<int, int, int, int, int>;
 std::mutex gTuneMutex;
-std::map<std::tuple<int, int, int, int, int>, std::pair<int, int>> gTuneCache;
+std::map<TuneKey, std::pair<int, int>> gTuneCache;
+
+// Persistent tune cache: HPHC_TUNE_CACHE names a file of JSON lines, one per
+// tuned shape,
+//   {"v":1,"device":"<name>","sms":148,"D":2,"precision":1,"mode":50,
+//    "pairs_log2":34,"problems_log2":0,"R":4,"items":64}
+// read once per process (lines of other devices, other versions or with an
+// invalid shape are ignored) and appended to after each new tuning.  Each
+// line is written with one append of under 200 bytes, so processes sharing
+// the file do not interleave their lines.
+constexpr int kTuneCacheVersion = 1;
+
+struct TuneLine {
+    std::string device;
+    int sms;
+    TuneKey key;
+    int R, items;
+};
+std::vector<TuneLine> gTuneFile;
+bool gTuneFileRead = false;
+
+// Position of the value of "key" in a one-line JSON object (after the
+// colon and any blanks), or npos.
+size_t json_value(const std::string& line, const char* key) {
+    const std::string k = std::string("\"") + key + "\"";
+    size_t at = line.find(k);
+    if (at == std::string::npos) return at;
+    at = line.find_first_not_of(" \t", at + k.size());
+    if (at == std::string::npos || line[at] != ':') return std::string::npos;
+    return line.find_first_not_of(" \t", at + 1);
+}
+
+bool json_int(const std::string& line, const char* key, int* out) {
+    const size_t at = json_value(line, key);
+    if (at == std::string::npos) return false;
+    char* end = nullptr;
+    const long v = std::strtol(line.c_str() + at, &end, 10);
+    if (end == line.c_str() + at) return false;
+    *out = (int)v;
+    return true;
+}
+
+bool json_string(const std::string& line, const char* key, std::string* out) {
+    const size_t at = json_value(line, key);
+    if (at == std::string::npos || line[at] != '"') return false;
+    const size_t end = line.find('"', at + 1);
+    if (end == std::string::npos) return false;
+    *out = line.substr(at + 1, end - at - 1);
+    return true;
+}
+
+bool valid_shape(int precision, int R, int items) {
+    const bool okR = precision == HPHC_PRECISION_FP64 ? (R == 1 || R == 2) : (R == 2 || R == 4);
+    return okR && items >= 1 && items <= 1024;
+}
+
+// Called with gTuneMutex held.
+void read_tune_file() {
+    if (gTuneFileRead) return;
+    gTuneFileRead = true;
+    const char* path = std::getenv("HPHC_TUNE_CACHE");
+    if (!path || !*path) return;
+    FILE* f = std::fopen(path, "r");
+    if (!f) return;
+    char buf[512];
+    while (std::fgets(buf, sizeof buf, f)) {
+        const std::string line(buf);
+        TuneLine t;
+        int v = 0, D = 0, prec = 0, mode = 0, pb = 0, kb = 0;
+        if (!json_int(line, "v", &v) || v != kTuneCacheVersion) continue;
+        if (!json_string(line, "device", &t.device) || !json_int(line, "sms", &t.sms) ||
+            !json_int(line, "D", &D) || !json_int(line, "precision", &prec) ||
+            !json_int(line, "mode", &mode) || !json_int(line, "pairs_log2", &pb) ||
+            !json_int(line, "problems_log2", &kb) || !json_int(line, "R", &t.R) ||
+            !json_int(line, "items", &t.items))
+            continue;
+        if (!valid_shape(prec, t.R, t.items)) continue;
+        t.key = std::make_tuple(D, prec, mode, pb, kb);
+        gTuneFile.push_back(t);
+    }
+    std::fclose(f);
+}
+
+void append_tune_file(const std::string& device, int sms, const TuneKey& key, int R, int items) {
+    const char* path = std::getenv("HPHC_TUNE_CACHE");
+    if (!path || !*path) return;
+    std::string name = device;
+    for (char& ch : name)
+        if (ch == '"' || ch == '\\' || (unsigned char)ch < 0x20) ch = '_';
+    char line[400];
+    const int n = std::snprintf(
+        line, sizeof line,
+        "{\"v\":%d,\"device\":\"%s\",\"sms\":%d,\"D\":%d,\"precision\":%d,\"mode\":%d,"
+        "\"pairs_log2\":%d,\"problems_log2\":%d,\"R\":%d,\"items\":%d}\n",
+        kTuneCacheVersion, name.c_str(), sms, std::get<0>(key), std::get<1>(key),
+        std::get<2>(key), std::get<3>(key), std::get<4>(key), R, items);
+    if (n <= 0 || n >= (int)sizeof line) return;
+    FILE* f = std::fopen(path, "a");
+    if (!f) return;
+    std::fwrite(line, 1, (size_t)n, f);
+    std::fclose(f);
+}
 
 int log2_bucket(double x) {
     int b = 0;
@@ -523,11 +629,23 @@ int Executor::autotune(const std::vector<SetView>& sets, const int* setOf, const
     double pairs = 0.0;
     for (int p = 0; p < P; ++p) pairs += (double)sets[setOf[p]].N * sets[setOf[p]].N;
     pairs /= std::max(1, shardWorld);  // work of this rank
-    const auto key = std::make_tuple(D_, precision_, variant_ | (symmetric ? 16 : 0),
-                                     log2_bucket(pairs), log2_bucket(P));
+    const int mode = variant_ | (symmetric ? 16 : 0) | (fastTail ? 32 : 0) | (skip_ ? 64 : 0);
+    const TuneKey key = std::make_tuple(D_, precision_, mode, log2_bucket(pairs), log2_bucket(P));
+    if (deviceName_.empty()) {
+        cudaDeviceProp prop{};
+        deviceName_ = cudaGetDeviceProperties(&prop, device_) == cudaSuccess ? prop.name : "?";
+    }
     {
         std::lock_guard<std::mutex> lock(gTuneMutex);
         auto it = gTuneCache.find(key);
+        if (it == gTuneCache.end()) {
+            read_tune_file();
+            for (const TuneLine& t : gTuneFile)
+                if (t.key == key && t.sms == numSMs_ && t.device == deviceName_) {
+                    it = gTuneCache.emplace(key, std::make_pair(t.R, t.items)).first;
+                    break;
+                }
+        }
         if (it != gTuneCache.end()) {
             R = fixedR ? fixedR : it->second.first;
             itemsPerSM = fixedItems ? fixedItems : it->second.second;
@@ -576,9 +694,10 @@ int Executor::autotune(const std::vector<SetView>& sets, const int* setOf, const
     }
     kernelTiming = timing;
     if (st) return st;
-    {
+    if (!fixedR && !fixedItems) {  // a shape tuned under a constraint is not cached
         std::lock_guard<std::mutex> lock(gTuneMutex);
         gTuneCache[key] = {bestR, bestI};
+        append_tune_file(deviceName_, numSMs_, key, bestR, bestI);
     }
     R = bestR;
     itemsPerSM = bestI;
@@ -650,6 +769,8 @@ int Executor::enqueue(const std::vector<SetView>& sets, const int* setOf, const 
         }
         graphKey_ = key;
     }
+    if (take_fault(HPHC_FAULT_LAUNCH))
+        return cuda_fail(cudaErrorLaunchOutOfResources, "launch graph (injected)");
     if ((e = cudaGraphLaunch(graphExec_, stream_))) return cuda_fail(e, "launch graph");
     lastLaunches = (precision_ == HPHC_PRECISION_FP64 ? 3 : 4);
     timedValid = kernelTiming;
@@ -659,6 +780,10 @@ int Executor::enqueue(const std::vector<SetView>& sets, const int* setOf, const 
 int Executor::wait(double* hostOut) {
     const cudaError_t e = cudaStreamSynchronize(stream_);
     if (e != cudaSuccess) return cuda_fail(e, "evaluation");
+    if (take_fault(HPHC_FAULT_WAIT)) {
+        timedValid = false;
+        return cuda_fail(cudaErrorLaunchTimeout, "evaluation (injected)");
+    }
     if (hostOut) std::memcpy(hostOut, hOut_, (size_t)plan_.P * 8 * sizeof(double));
     if (timedValid) {
         cudaError_t t;

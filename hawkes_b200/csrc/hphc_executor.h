@@ -102,6 +102,14 @@ public:
     // are then this rank's share; the shares of all ranks add up to the sums
     // of the unsharded sweep.
     int shardRank = 0, shardWorld = 1;
+    // Fault injection (HPHC_FAULT_LAUNCH / HPHC_FAULT_WAIT): the next
+    // faultCount launches or waits fail with a stand-in error.
+    int faultStage = 0, faultCount = 0;
+    bool take_fault(int stage) {
+        if (faultStage != stage || faultCount <= 0) return false;
+        if (--faultCount == 0) faultStage = 0;
+        return true;
+    }
     double* sumsOut = nullptr;  // if set, problem 0's unit pair sums ([6][N], natural units)
     float lastSweepMs = 0.f, lastFinishMs = 0.f, lastStepMs = 0.f;
     bool timedValid = false;
@@ -113,6 +121,7 @@ private:
     bool wideBands_ = false;  // build_plan: bands for any sampled parameters
     int loopGrid_ = 0;        // sweep grid of the device loop
     double ex2Bias_ = 0.0;
+    std::string deviceName_;  // for the persistent tune cache
     cudaStream_t stream_ = nullptr;
     bool tuned_ = false;
 

@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <string>
 
@@ -11,6 +12,15 @@
 #include "hphc_kernels.cuh"
 
 namespace hphc {
+
+// NVTX range over a scope (header-only NVTX v3: a no-op unless a profiler
+// is attached), so timelines and ncu --nvtx filters see the engine's phases.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // What the device-resident loop needs from an engine after set-up.
 struct EngineLoop {

@@ -217,6 +217,7 @@ int hphc_sampler_run(hphc_sampler* s, hphc_engine* engine, int iterations, int b
     if (!engine) return s->fail(HPHC_ERR_INVALID_HANDLE, "null engine");
     if (iterations < 0 || burnIn < 0 || burnIn > iterations)
         return s->fail(HPHC_ERR_BAD_ARGUMENT, "iterations %d, burnIn %d", iterations, burnIn);
+    hphc::NvtxRange range("hphc sampler run (host driver)");
     auto eval = [&](const double* p, int K, double* ll) -> int {
         const int st = hphc_batch_log_likelihood_and_gradient(engine, p, K, ll, nullptr);
         if (st) s->fail(st, "likelihood evaluation: %s", hphc_last_error(engine));
@@ -250,6 +251,7 @@ int hphc_sampler_run_device(hphc_sampler* s, hphc_engine* engine, int iterations
             return s->fail(HPHC_ERR_UNSUPPORTED,
                            "the device driver keeps tauXprec and tauTprec fixed (they set the "
                            "record scaling and the work list); use hphc_sampler_run");
+    hphc::NvtxRange range("hphc sampler run (device driver)");
     auto eval = [&](const double* p, int K, double* ll) -> int {
         const int st = hphc_batch_log_likelihood_and_gradient(engine, p, K, ll, nullptr);
         if (st) s->fail(st, "likelihood evaluation: %s", hphc_last_error(engine));

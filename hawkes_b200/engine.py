@@ -51,6 +51,11 @@ FP32_ORDERED = ORDERED  # earlier name of the same bit
 NO_INCREMENTAL = 1 << 14
 NO_FAST_TAIL = 1 << 15  # FP32-compensated: polynomial exponential for the far tail too
 
+# Fault-injection stages (CudaHawkes.injectFault).
+FAULT_UPLOAD = 1
+FAULT_LAUNCH = 2
+FAULT_WAIT = 3
+
 # How an evaluation was computed (CudaHawkes.lastEvaluationPath).
 PATH_SWEEP = 0
 PATH_INCREMENTAL = 1
@@ -251,6 +256,12 @@ class CudaHawkes:
         v = ctypes.c_double()
         self._check(_lib.hphc_get_last_launch_evals(self._h, ctypes.byref(v)), "lastLaunchEvals")
         return v.value
+
+    def injectFault(self, stage: int, count: int = 1) -> None:
+        """Make the next `count` calls that reach `stage` (FAULT_UPLOAD,
+        FAULT_LAUNCH, FAULT_WAIT) fail there with a stand-in CUDA error; the
+        engine stays usable.  count 0 clears."""
+        self._check(_lib.hphc_inject_fault(self._h, int(stage), int(count)), "injectFault")
 
     # -- sharded evaluation (hawkes_b200.shard) --------------------------------
     def sweepShard(self, rank: int, world: int, devicePart: int) -> None:

@@ -81,8 +81,8 @@ extern "C" {
 #define HPHC_FLAG_NO_FAST_TAIL (1L << 15)    /* FP32-compensated mode: the polynomial
                                                 exponential for every pair term (by default
                                                 tile pairs whose background terms are all
-                                                below 2^-12 of an event's own term, and that
-                                                hold no self-excitation term, use ex2.approx) */
+                                                below 2^-12 of an event's own term take those
+                                                terms from ex2.approx) */
 
 /* How the last evaluation was computed (hphc_get_last_evaluation_path). */
 #define HPHC_PATH_SWEEP 0        /* the O(N^2) pair sweep                             */
@@ -327,6 +327,20 @@ int hphc_sweep_shard(hphc_engine* engine, int rank, int world, double* devicePar
  * engine's own hphc_sweep_shard. */
 int hphc_set_unit_sums(hphc_engine* engine, const double* deviceParts, int numParts,
                        size_t length);
+
+/* ---- fault injection (testing) --------------------------------------------
+ * No reference counterpart.  Makes error handling testable without a GPU
+ * fault: the next `count` calls of this handle that reach `stage` fail there
+ * with a stand-in CUDA error instead of making the CUDA call (nothing is
+ * uploaded or launched at that stage; at HPHC_FAULT_WAIT the launched work is
+ * waited for first).  The call returns the status that error maps to, with
+ * "injected" in hphc_last_error; the engine stays usable and its next calls
+ * run normally.  count 0 clears.  Sampler runs on the engine see the same
+ * faults. */
+#define HPHC_FAULT_UPLOAD 1 /* host-to-device upload of events (HPHC_ERR_OUT_OF_MEMORY) */
+#define HPHC_FAULT_LAUNCH 2 /* graph or kernel launch of an evaluation (HPHC_ERR_CUDA)  */
+#define HPHC_FAULT_WAIT 3   /* completion wait of an evaluation (HPHC_ERR_CUDA)         */
+int hphc_inject_fault(hphc_engine* engine, int stage, int count);
 
 /* ---- introspection and device-resident timing --------------------------- */
 
