@@ -490,11 +490,25 @@ struct hphc_engine {
         return HPHC_OK;
     }
 
-    // Enqueue K parameter vectors on this engine's events (full sweep).
-    int enqueue(const double* p, int K, bool wantProbs) {
+    // The kept background sums serve parameter vectors p (K x 6) when every
+    // one has the kept tauX and tauT: the background unit sums depend on the
+    // events and those two parameters only.  With no moved event the sums
+    // describe the host copy of the events, which enqueue uploads if needed.
+    bool kept_background_serves(const double* p, int K) const {
+        if (!incremental || !sumsValid || pendingSums || !moved.empty()) return false;
+        for (int k = 0; k < K; ++k)
+            if (p[6 * k + 1] != sumsParams[1] || p[6 * k + 2] != sumsParams[2]) return false;
+        return true;
+    }
+
+    // Enqueue K parameter vectors on this engine's events: the full sweep, or
+    // (reuse) only the self-excitation terms when the kept background sums
+    // serve.
+    int enqueue(const double* p, int K, bool wantProbs, bool reuse = true) {
         NvtxRange range("hphc sweep enqueue");
         lastLaunches = 0;
-        lastPath = HPHC_PATH_SWEEP;
+        const bool selfOnly = reuse && kept_background_serves(p, K);
+        lastPath = selfOnly ? HPHC_PATH_SELF_EXCITATION : HPHC_PATH_SWEEP;
         // moved events are only on the host, and after incremental row uploads
         // the packed FP64 records are stale: upload and pack everything (the
         // kept sums and the moved list stay a consistent pair)
@@ -503,15 +517,18 @@ struct hphc_engine {
         if (st) return st;
         std::vector<SetView> sets{set.view()};
         std::vector<int> setOf(K, 0);
-        // a single evaluation keeps its sums for later incremental updates
-        pendingSums = incremental && K == 1;
+        // the evaluation keeps problem 0's sums (a self-excitation-only sweep
+        // rewrites rows 3-5 and keeps rows 0-2)
+        pendingSums = incremental;
         rt.ex.sumsOut = pendingSums ? dSums.p : nullptr;
+        rt.ex.keptB = selfOnly ? dSums.p : nullptr;
         if (pendingSums) {
             invalidate_sums();
             std::memcpy(pendingSumsParams, p, sizeof pendingSumsParams);
         }
         st = rt.ex.enqueue(sets, setOf.data(), p, K, wantProbs ? dProbs.p : nullptr);
         rt.ex.sumsOut = nullptr;
+        rt.ex.keptB = nullptr;
         if (st) {
             pendingSums = false;
             return fmt(lastError, st, "%s", rt.ex.error.c_str());
@@ -535,9 +552,11 @@ struct hphc_engine {
         return HPHC_OK;
     }
 
+    // The kept sums serve p in full when sigma, tauX, tauT and omega are the
+    // kept ones (theta and mu0 enter only the finish).
     bool can_update(const double* p) const {
         return incremental && sumsValid && !pendingSums &&
-               std::memcmp(p, sumsParams, sizeof sumsParams) == 0;
+               std::memcmp(p, sumsParams, 4 * sizeof(double)) == 0;
     }
 
     // O(N) evaluation from the kept sums: upload and apply each moved event,
@@ -711,12 +730,17 @@ int hphc::engine_loop_setup(hphc_engine* e, const double* params, int K, EngineL
     if (st) return fmt(*err, st, "%s", e->lastError.c_str());
     std::vector<SetView> sets{e->set.view()};
     std::vector<int> setOf(K, 0);
+    // Chains that all have the kept sums' tauX and tauT (the loop keeps them
+    // fixed) reuse the kept background sums in every iteration and sweep only
+    // the self-excitation terms.  The loop does not write the kept sums.
+    e->rt.ex.keptB = e->kept_background_serves(params, K) ? e->dSums.p : nullptr;
     st = e->rt.ex.setup_device_loop(sets, setOf.data(), params, K);
+    out->spec = e->rt.ex.consts_spec();
+    e->rt.ex.keptB = nullptr;
     if (st) return fmt(*err, st, "%s", e->rt.ex.error.c_str());
     out->device = e->rt.device;
     out->stream = e->rt.stream;
     out->ex = &e->rt.ex;
-    out->spec = e->rt.ex.consts_spec();
     return HPHC_OK;
 }
 
@@ -959,7 +983,7 @@ int hphc_enqueue_log_likelihood_and_gradient(hphc_engine* e) {
     if (!e) return HPHC_ERR_INVALID_HANDLE;
     DeviceGuard g(e->rt.device);
     if (!g.ok) return e->fail(HPHC_ERR_CUDA, "cannot select device %d", e->rt.device);
-    return e->enqueue(e->params, 1, false);
+    return e->enqueue(e->params, 1, false, /*reuse=*/false);  // always the full sweep
 }
 
 int hphc_read_results(hphc_engine* e, double* loglik, double* gradient, size_t length) {
@@ -1044,7 +1068,7 @@ int hphc_get_last_launch_stats(hphc_engine* e, int* kernelLaunches, double* back
                                double* selfExciteTerms) {
     if (!e) return HPHC_ERR_INVALID_HANDLE;
     if (kernelLaunches) *kernelLaunches = e->lastLaunches;
-    if (e->lastPath != HPHC_PATH_SWEEP) {
+    if (e->lastPath == HPHC_PATH_INCREMENTAL || e->lastPath == HPHC_PATH_KEPT_SUMS) {
         // per moved event: its pair with every other event at the old and the
         // new location, and its new row
         if (backgroundTerms) *backgroundTerms = e->lastIncTerms;
@@ -1064,7 +1088,7 @@ int hphc_get_last_launch_stats(hphc_engine* e, int* kernelLaunches, double* back
 int hphc_get_last_launch_evals(hphc_engine* e, double* backgroundEvals) {
     if (!e) return HPHC_ERR_INVALID_HANDLE;
     if (!backgroundEvals) return HPHC_ERR_BAD_ARGUMENT;
-    if (e->lastPath != HPHC_PATH_SWEEP) {
+    if (e->lastPath == HPHC_PATH_INCREMENTAL || e->lastPath == HPHC_PATH_KEPT_SUMS) {
         *backgroundEvals = e->lastIncTerms;
         return HPHC_OK;
     }

@@ -32,7 +32,7 @@ void tile_needs(double tminI, double tmaxI, double tminJ, double tmaxJ, const Pa
                 bool* doB, bool* doS) {
     const double dtLo = tminI - tmaxJ, dtHi = tmaxI - tminJ;
     const double minAbs = dtLo > 0.0 ? dtLo : (dtHi < 0.0 ? -dtHi : 0.0);
-    *doB = !(c.skipB >= 0.0 && -c.cB * minAbs * minAbs >= c.skipB);
+    *doB = !c.noB && !(c.skipB >= 0.0 && -c.cB * minAbs * minAbs >= c.skipB);
     const bool allCausal = dtLo > 0.0;
     *doS = (dtHi > 0.0) && !(c.skipS >= 0.0 && allCausal && -c.cW * dtLo >= c.skipS);
 }
@@ -219,6 +219,7 @@ ConstsSpec Executor::consts_spec() const {
     s.skip = skip_ ? 1 : 0;
     s.ex2Bias = ex2Bias_;
     s.fastTail = fastTail ? 1 : 0;
+    s.noB = keptB ? 1 : 0;
     return s;
 }
 
@@ -302,7 +303,8 @@ int Executor::build_plan(const std::vector<SetView>& sets, const int* setOf, con
         sp.tileMax = s.dTileMax;
         sp.partials = reinterpret_cast<double*>(partOff);  // offset, fixed up later
         partOff += (size_t)maxChunks * kNumAcc * Npad;
-        sp.symmetric = (symmetric && N <= kMaxSymmetricEvents) ? 1 : 0;
+        // a self-excitation-only sweep has no background, so no column sums
+        sp.symmetric = (symmetric && !keptB && N <= kMaxSymmetricEvents) ? 1 : 0;
         if (!fp32 && sp.symmetric) {
             // FP64 column sums are fixed point: bound each column total by N
             // times the largest term, B_u <= 1, B_u d^2 <= 1/(e |cA|),
@@ -436,6 +438,7 @@ int Executor::build_plan(const std::vector<SetView>& sets, const int* setOf, con
         fp.times = s.dTimes;
         fp.probs = (p == 0) ? dProbs : nullptr;
         fp.sums = (p == 0) ? sumsOut : nullptr;
+        fp.keptB = keptB;
         fp.N = N;
         fp.Npad = Npad;
         fp.stripEvents = stripEvents;

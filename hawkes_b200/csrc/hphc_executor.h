@@ -111,6 +111,12 @@ public:
         return true;
     }
     double* sumsOut = nullptr;  // if set, problem 0's unit pair sums ([6][N], natural units)
+    // If set: a self-excitation-only sweep.  keptB holds the background unit
+    // sums ([3][N], natural units) of an earlier sweep of the same single
+    // event set at the same tauX and tauT as every problem of this run (the
+    // caller checks that); the finish uses them and the sweep evaluates no
+    // background term.  Rows 0-2 of sumsOut are then not written.
+    const double* keptB = nullptr;
     float lastSweepMs = 0.f, lastFinishMs = 0.f, lastStepMs = 0.f;
     bool timedValid = false;
     int lastLaunches = 0;

@@ -120,7 +120,7 @@ __device__ __forceinline__ TileMode tile_mode(double tminI, double tmaxI, double
     const double dtLo = tminI - tmaxJ, dtHi = tmaxI - tminJ;
     const double minAbs = dtLo > 0.0 ? dtLo : (dtHi < 0.0 ? -dtHi : 0.0);
     TileMode m;
-    m.doB = !(c.skipB >= 0.0 && -c.cB * minAbs * minAbs >= c.skipB);
+    m.doB = !c.noB && !(c.skipB >= 0.0 && -c.cB * minAbs * minAbs >= c.skipB);
     m.allCausal = dtLo > 0.0;
     const bool anyCausal = dtHi > 0.0;
     m.doS = anyCausal && !(c.skipS >= 0.0 && m.allCausal && -c.cW * dtLo >= c.skipS);
@@ -1027,8 +1027,12 @@ finish_list_kernel(const FinishProblem* __restrict__ problems,
                 else
                     acc += (double)P.colAcc[(size_t)q * P.Npad + i] * kColInv;
             }
-            s[q] = acc * f.accScale[q];
-            if (P.sums) P.sums[(size_t)q * N + i] = s[q];
+            if (q < 3 && P.keptB) {
+                s[q] = P.keptB[(size_t)q * N + i];  // unchanged: not written back
+            } else {
+                s[q] = acc * f.accScale[q];
+                if (P.sums) P.sums[(size_t)q * N + i] = s[q];
+            }
         }
         event_contributions(f, s, P.times[i], v, P.probs ? P.probs + i : nullptr);
     }

@@ -51,6 +51,10 @@ struct PairConsts {
     // exp(-fastB) (natural log; < 0 disables) takes them from the hardware
     // exponential (see kFastTailLog2).
     double fastB;
+    // Self-excitation-only sweep: no background term is evaluated (the
+    // finish takes the background sums from an earlier sweep, which depend
+    // on tauX and tauT only).
+    int noB, pad;
 };
 
 // Constants of the per-event finish (all FP64).
@@ -77,6 +81,7 @@ struct ConstsSpec {
     int skip;         // tile-level underflow skip on
     double ex2Bias;   // mean relative error of ex2.approx (hardware-exponential variant)
     int fastTail;     // FP32 software-exponential variant: far tile pairs use the hardware one
+    int noB;          // self-excitation-only sweep (PairConsts::noB)
 };
 
 // Far background tail of the FP32 software-exponential mode.  A tile pair
@@ -132,6 +137,8 @@ inline void param_consts(const double* p, const ConstsSpec& s, PairConsts& c, Fi
     c.fastB = (fp32 && s.fastTail && (s.variant & 2) && c.cB < 0.0 && c.cA <= 0.0)
                   ? kFastTailLog2 * kLn2
                   : -1.0;
+    c.noB = s.noB;
+    c.pad = 0;
 
     double aD = 1.0, sigmaD = 1.0;
     for (int k = 0; k < s.D; ++k) {
@@ -260,6 +267,9 @@ struct FinishProblem {
     const double* times;      // the set's raw times
     double* probs;            // P_i output (may be null)
     double* sums;             // [6][N] unit pair sums out, natural units (may be null)
+    const double* keptB;      // [3][N] background unit sums (natural units) of an earlier
+                              // sweep on the same events and tauX, tauT, used instead of
+                              // this sweep's (which then has no background terms), or null
     int N, Npad, stripEvents, blockBase;  // blockBase: first finish CTA of this problem
     int nBlocks, colWords, pad0, pad1;    // colWords: 1 = FP32 column format, 2 = FP64
     int colShift[4];

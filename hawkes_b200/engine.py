@@ -60,6 +60,7 @@ FAULT_WAIT = 3
 PATH_SWEEP = 0
 PATH_INCREMENTAL = 1
 PATH_KEPT_SUMS = 2
+PATH_SELF_EXCITATION = 3
 
 PRECISION_FP64 = 0
 PRECISION_FP32_COMP = 1

@@ -88,6 +88,8 @@ extern "C" {
 #define HPHC_PATH_SWEEP 0        /* the O(N^2) pair sweep                             */
 #define HPHC_PATH_INCREMENTAL 1  /* kept sums updated for moved events, O(N) each     */
 #define HPHC_PATH_KEPT_SUMS 2    /* nothing changed since the sums were kept: O(N) finish */
+#define HPHC_PATH_SELF_EXCITATION 3 /* kept background sums (same events, tauX, tauT):
+                                       only the self-excitation terms swept */
 
 /* Precision modes reported by hphc_get_precision(). */
 #define HPHC_PRECISION_FP64 0          /* plain FP64 pair terms and reductions           */
@@ -353,7 +355,8 @@ int hphc_get_stream(hphc_engine* engine, void** stream);
 
 /* Enqueue one log-likelihood + gradient evaluation on the engine's stream
  * with the data already on the device, without waiting and without copying
- * results back.  hphc_read_results() waits and returns them. */
+ * results back.  hphc_read_results() waits and returns them.  Always the full
+ * pair sweep (no kept sums are reused), so that it times the whole work. */
 int hphc_enqueue_log_likelihood_and_gradient(hphc_engine* engine);
 
 /* Wait for the last enqueued evaluation and copy its log-likelihood and
@@ -363,14 +366,26 @@ int hphc_read_results(hphc_engine* engine, double* loglik, double* gradient, siz
 /* Which path the most recent single evaluation took (HPHC_PATH_*).
  * Incremental evaluation (no reference counterpart; the reference recomputes
  * the O(N^2) sum on every call): after an evaluation the engine keeps each
- * event's six unit pair sums.  If only a few events then move
- * (hphc_update_locations with an index; at most max(1, min(64, N/512)) since
- * the sums were formed) and the parameters are the same, the next evaluation
- * updates every event's sums by its pair with each moved event and recomputes
- * the moved events' own rows, O(N) per moved event, then re-runs the O(N)
- * finish.  Changing the times, all locations (index -1) or moving more events
- * falls back to the sweep.  Results agree with the sweep to FP64 rounding of
- * the updates (FP64 mode) or to the FP32 mode's own accuracy. */
+ * event's six unit pair sums (of parameter vector 0 for a batched call).  The
+ * background sums depend only on the events, tauX and tauT, the
+ * self-excitation sums only on the events, sigma and omega; theta and mu0
+ * enter only the O(N) finish.  So:
+ *   - same sigma, tauX, tauT, omega (theta, mu0 free), no event moved:
+ *     the O(N) finish only (HPHC_PATH_KEPT_SUMS);
+ *   - the same, after a few events moved (hphc_update_locations with an
+ *     index; at most max(1, min(64, N/512)) since the sums were formed):
+ *     every event's sums are updated by its pair with each moved event and
+ *     the moved events' rows recomputed, O(N) per moved event, then the
+ *     finish (HPHC_PATH_INCREMENTAL);
+ *   - same tauX and tauT in every parameter vector, sigma or omega changed,
+ *     no event moved: only the self-excitation terms are swept (a narrow band
+ *     near the diagonal for sorted times) and the kept background sums are
+ *     reused (HPHC_PATH_SELF_EXCITATION) -- the steps of the reference's
+ *     sampler, which keeps tauX and tauT fixed;
+ *   - otherwise the full sweep (HPHC_PATH_SWEEP).
+ * Changing the times or all locations (index -1) forces the sweep.  Results
+ * agree with the sweep to FP64 rounding (FP64 mode) or to the FP32 mode's own
+ * accuracy.  HPHC_FLAG_NO_INCREMENTAL keeps no sums. */
 int hphc_get_last_evaluation_path(hphc_engine* engine, int* path);
 
 /* Kernel launches made by the most recent evaluation call (for launch

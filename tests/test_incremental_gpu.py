@@ -111,7 +111,7 @@ def test_fallbacks_to_the_sweep():
         e.setTimesData(t2)
         check(e, loc, t2, q, FP64)
         assert e.lastEvaluationPath == hb.PATH_SWEEP
-        # a batch does not disturb the kept sums
+        # a batch keeps its first parameter vector's sums (here the engine's own)
         e.batchLogLikelihoodAndGradient(np.stack([q, p]))
         e.getSumOfLikContribs()
         assert e.lastEvaluationPath == hb.PATH_KEPT_SUMS
