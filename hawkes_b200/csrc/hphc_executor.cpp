@@ -322,6 +322,7 @@ int Executor::build_plan(const std::vector<SetView>& sets, const int* setOf, con
                 }
             }
         }
+        sp.searchBand = (wideBands_ && s.sorted) ? 1 : 0;
         sp.colAcc = nullptr;
         if (sp.symmetric) {
             sp.colAcc = reinterpret_cast<unsigned long long*>(colOff + 1);  // offset + 1
@@ -426,6 +427,7 @@ int Executor::build_plan(const std::vector<SetView>& sets, const int* setOf, con
                 w.jt0 = std::max(lo, c * CT);
                 w.jt1 = std::min(hi, (c + 1) * CT);
                 w.slot = c - cFirst;
+                w.start = w.jt0;
                 pl.items.push_back(w);
             }
             pl.stripChunks.push_back(cLast - cFirst);
@@ -838,13 +840,17 @@ int Executor::enqueue_device_body() {
     const int prec = precision_ == HPHC_PRECISION_FP64 ? 0 : 1;
     char* d = static_cast<char*>(dTables_);
     const auto* sp = reinterpret_cast<const SweepProblem*>(d + offSP_);
-    const auto* items = reinterpret_cast<const WorkItem*>(d + offItems_);
+    auto* items = reinterpret_cast<WorkItem*>(d + offItems_);
     const auto* nItems = reinterpret_cast<const int*>(d + offNItems_);
     const auto* fp = reinterpret_cast<const FinishProblem*>(d + offFP_);
     const auto* fb = reinterpret_cast<const FinishBlock*>(d + offFB_);
     cudaError_t e;
     if ((e = cudaMemsetAsync(dCounter_, 0, sizeof(int), stream_)))
         return cuda_fail(e, "reset work counter");
+    // the plan lists every earlier tile for any sigma and omega: start each
+    // item where the current constants allow a term
+    if ((e = launch_band_starts((int)plan_.items.size(), sp, items, nItems, R, stream_)))
+        return cuda_fail(e, "band kernel");
     if (colNeed_ && (e = cudaMemsetAsync(dColAcc_, 0, colNeed_ * sizeof(unsigned long long),
                                          stream_)))
         return cuda_fail(e, "reset column sums");
@@ -855,7 +861,7 @@ int Executor::enqueue_device_body() {
         return cuda_fail(e, "finish kernel");
     if ((e = launch_final_list(plan_.P, fp, dBlockSums_, dOut_, stream_)))
         return cuda_fail(e, "final kernel");
-    lastLaunches = 3;
+    lastLaunches = 4;
     return HPHC_OK;
 }
 

@@ -279,6 +279,50 @@ __device__ __forceinline__ void tile_sym_f64(const double* __restrict__ sRec,
     }
 }
 
+// Where an item of a problem with searchBand set may start: the first tile
+// in [jt0, min(jt1, strip's first tile)) that is not ruled out by its time
+// gap to strip `strip` (R tiles of targets).  With sorted times the gap
+// shrinks as jt grows, so "the background can be non-zero, or the gap does
+// not make every self-excitation term underflow" turns on once and stays
+// on, and bisection finds the start with ~log2(nTiles) reads of the tile
+// bounds instead of one read per skipped tile.  The set it keeps contains
+// every tile tile_mode would evaluate (its causality test only removes more),
+// and the item still decides each tile with tile_mode.
+__device__ __forceinline__ int first_tile_with_terms(const SweepProblem& P, int R, int strip,
+                                                     int jt0, int jt1) {
+    const int ts0 = strip * R, ts1 = min(ts0 + R, P.nTiles);
+    double tminI = INFINITY, tmaxI = -INFINITY;
+    for (int t = ts0; t < ts1; ++t) {
+        tminI = fmin(tminI, P.tileMin[t]);
+        tmaxI = fmax(tmaxI, P.tileMax[t]);
+    }
+    int lo = jt0, hi = min(jt1, ts0);
+    while (lo < hi) {
+        const int mid = (lo + hi) / 2;
+        const TileMode m = tile_mode(tminI, tmaxI, P.tileMin[mid], P.tileMax[mid], P.c);
+        const double dtLo = tminI - P.tileMax[mid];
+        const bool sFar = P.c.skipS >= 0.0 && dtLo > 0.0 && -P.c.cW * dtLo >= P.c.skipS;
+        if (m.doB || !sFar)
+            hi = mid;
+        else
+            lo = mid + 1;
+    }
+    return lo;
+}
+
+// Device-resident loop: before each sweep, one thread per work item sets the
+// item's first tile from the problem's current constants (a separate launch,
+// so the sweep kernels themselves only read WorkItem::start).
+__global__ void __launch_bounds__(kBandThreads)
+band_starts_kernel(const SweepProblem* __restrict__ problems, WorkItem* __restrict__ items,
+                   const int* __restrict__ nItems, int R) {
+    const int it = blockIdx.x * kBandThreads + threadIdx.x;
+    if (it >= *nItems) return;
+    WorkItem w = items[it];
+    const SweepProblem& P = problems[w.problem];
+    items[it].start = P.searchBand ? first_tile_with_terms(P, R, w.strip, w.jt0, w.jt1) : w.jt0;
+}
+
 // One work item of the FP64 sweep: target strip `strip` (kSweepThreads * R
 // events) against j tiles [jt0, jt1); unit pair sums to partial slot `slot`.
 // sym: tiles before the strip are evaluated once per pair (rows + columns).
@@ -412,7 +456,7 @@ sweep_f64_list_kernel(const SweepProblem* __restrict__ problems,
         const PairConsts c = P.c;
         const int shift[3] = {P.colShift[0], P.colShift[1], P.colShift[2]};
         f64_item<D, R>(static_cast<const double*>(P.rec), P.tileMin, P.tileMax, P.partials, P.N,
-                       P.nTiles, P.Npad, c, w.strip, w.jt0, w.jt1, w.slot, sRec,
+                       P.nTiles, P.Npad, c, w.strip, w.start, w.jt1, w.slot, sRec,
                        P.symmetric != 0, P.colAcc, shift, sCol);
     }
 }
@@ -879,7 +923,7 @@ sweep_f32c_list_kernel(const SweepProblem* __restrict__ problems,
         const SweepProblem& P = problems[w.problem];
         const PairConsts c = P.c;
         f32c_item<D, R, V>(static_cast<const float*>(P.rec), P.tileMin, P.tileMax, P.partials,
-                           P.colAcc, P.N, P.nTiles, P.Npad, P.symmetric != 0, c, w.strip, w.jt0,
+                           P.colAcc, P.N, P.nTiles, P.Npad, P.symmetric != 0, c, w.strip, w.start,
                            w.jt1, w.slot, sTile, sCol);
     }
 }
@@ -1292,6 +1336,14 @@ cudaError_t launch_pack_f32_jobs(int D, int nJobs, int maxN, const PackJob* jobs
 #undef X
         default: return cudaErrorInvalidValue;
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_band_starts(int maxItems, const SweepProblem* problems, WorkItem* items,
+                               const int* nItems, int R, cudaStream_t s) {
+    if (maxItems <= 0) return cudaSuccess;
+    band_starts_kernel<<<(maxItems + kBandThreads - 1) / kBandThreads, kBandThreads, 0, s>>>(
+        problems, items, nItems, R);
     return cudaGetLastError();
 }
 

@@ -247,6 +247,10 @@ struct SweepProblem {
                                  // FP64 [3][2][Npad] two-word fixed point (see kColLoBits)
     int N, nTiles, Npad, symmetric;
     int colShift[4];        // FP64 column sums: fixed-point shift per weighted sum
+    // Items may start far before the first tile holding a term (plans built
+    // for any sigma and omega, sorted times): the sweep finds that tile by
+    // bisection on the tile time bounds instead of scanning to it.
+    int searchBand, pad[3];
     PairConsts c;
 };
 
@@ -254,10 +258,20 @@ struct SweepProblem {
 // tiles [jt0, jt1), written to partial-sum slot `slot` of that strip.  The
 // host lists items largest first; CTAs take them in that order from an atomic
 // counter, so slow and fast items balance across SMs, and every item writes
-// fixed slots, so results do not depend on which CTA ran it.
+// fixed slots, so results do not depend on which CTA ran it.  The sweep
+// starts at tile `start`: jt0, or in the device-resident loop the first tile
+// not ruled out by its time gap for the current constants (band_starts).
 struct WorkItem {
-    int problem, strip, jt0, jt1, slot, pad0, pad1, pad2;
+    int problem, strip, jt0, jt1, slot, start, pad1, pad2;
 };
+
+constexpr int kBandThreads = 256;
+
+// Device-resident loop: items[k].start for the first *nItems items (maxItems
+// bounds the grid), from each problem's current constants where searchBand is
+// set, else jt0.
+cudaError_t launch_band_starts(int maxItems, const SweepProblem* problems, WorkItem* items,
+                               const int* nItems, int R, cudaStream_t s);
 
 // Finish view of a problem.
 struct FinishProblem {

@@ -168,3 +168,38 @@ def test_samplers_with_fixed_tau_reuse_the_background(flags):
     np.testing.assert_allclose(sd, sh, rtol=1e-9)
     np.testing.assert_allclose(td, th, rtol=1e-8)
     assert np.all(acc > 0)
+
+
+@pytest.mark.parametrize("flags", [FP64, FP32C], ids=["fp64", "fp32c"])
+def test_device_loop_band_search_with_blocks_of_equal_times(flags):
+    # Times in blocks of 1280 equal values, 2 h apart: the tiles just before a
+    # strip share its time (no causal pair, no self-excitation term) while
+    # the block before them holds terms.  The device loop's plan lists every
+    # earlier tile and finds where to start by bisection on the tile time
+    # bounds; it must keep those earlier terms, as the host driver's
+    # host-planned bands do.
+    n = 6400
+    rng = np.random.default_rng(39)
+    loc = rng.uniform(0.0, 20.0, size=(n, 2))
+    t = (np.arange(n) // 1280) * 2.0
+    base = np.asarray(workloads.BASE_PARAMS, dtype=float)
+    z = rng.standard_normal((8, 6))
+    z[:, 1:3] = 0.0
+    init = base * np.exp(0.2 * z)
+    with _engine(loc, t, base, flags) as e:
+        with hb.Sampler(init, radius=0.4, seed=11) as a:
+            sh, th = a.run(e, 30, burnIn=2)
+        with hb.Sampler(init, radius=0.4, seed=11) as b:
+            sd, td = b.run(e, 30, burnIn=2, device=True)
+    np.testing.assert_allclose(sd, sh, rtol=1e-9)
+    np.testing.assert_allclose(td, th, rtol=1e-8)
+    # and with chains whose tauX, tauT differ (no kept background: the device
+    # loop sweeps both kinds of terms over its wide bands)
+    init2 = base * np.exp(0.2 * rng.standard_normal((8, 6)))
+    with _engine(loc, t, base, flags) as e:
+        with hb.Sampler(init2, radius=0.4, seed=12) as a:
+            sh, th = a.run(e, 20)
+        with hb.Sampler(init2, radius=0.4, seed=12) as b:
+            sd, td = b.run(e, 20, device=True)
+    np.testing.assert_allclose(sd, sh, rtol=1e-9)
+    np.testing.assert_allclose(td, th, rtol=1e-8)
