@@ -124,7 +124,8 @@ __device__ __forceinline__ TileMode tile_mode(double tminI, double tmaxI, double
     m.allCausal = dtLo > 0.0;
     const bool anyCausal = dtHi > 0.0;
     m.doS = anyCausal && !(c.skipS >= 0.0 && m.allCausal && -c.cW * dtLo >= c.skipS);
-    m.fastB = c.fastB >= 0.0 && -c.cB * minAbs * minAbs >= c.fastB;
+    // fastB > 0 when enabled (12 ln 2); zero-initialized constants keep it off
+    m.fastB = c.fastB > 0.0 && -c.cB * minAbs * minAbs >= c.fastB;
     return m;
 }
 
