@@ -203,3 +203,29 @@ def test_device_loop_band_search_with_blocks_of_equal_times(flags):
             sd, td = b.run(e, 20, device=True)
     np.testing.assert_allclose(sd, sh, rtol=1e-9)
     np.testing.assert_allclose(td, th, rtol=1e-8)
+
+
+@pytest.mark.parametrize("D", [1, 3])
+@pytest.mark.parametrize("flags", [FP64, FP32C], ids=["fp64", "fp32c"])
+def test_reuse_in_other_dimensions(flags, D):
+    loc, t = workloads.uniform(3000, seed=60 + D, D=D)
+    p = np.asarray(workloads.BASE_PARAMS, dtype=float).copy()
+    scale = oracle.oracle_eval(loc, t, p, threads=4)["grad_scale"]
+
+    def make(fl):
+        e = hb.CudaHawkes(D, len(t), fl, 0)
+        e.setTimesData(t)
+        e.updateLocations(-1, loc)
+        e.setParameters(p)
+        return e
+
+    with make(flags) as e, make(flags | hb.NO_INCREMENTAL) as ref:
+        e.getLogLikelihoodAndGradient()
+        for k, f in ((0, 1.2), (4, 0.8), (3, 1.3), (5, 1.1)):
+            p[k] *= f
+            e.setParameters(p)
+            ref.setParameters(p)
+            got = e.getLogLikelihoodAndGradient()
+            assert e.lastEvaluationPath == (hb.PATH_SELF_EXCITATION if k in (0, 3)
+                                            else hb.PATH_KEPT_SUMS)
+            _close(flags, got, ref.getLogLikelihoodAndGradient(), scale)
