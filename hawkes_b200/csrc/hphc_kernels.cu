@@ -485,8 +485,16 @@ sweep_f64_list_kernel(const SweepProblem* __restrict__ problems,
 //   kPolyExp  exponentials by exp2_poly_neg2 (unbiased to ~3e-10) instead of
 //             ex2.approx, whose measured mean relative error the finish
 //             divides out of the sums.
+//   kTimeHiOnly  background terms from the hi parts of the times only (far-tail
+//             tile pairs, set by the sweep itself): the lo parts are at most
+//             half an FP32 ulp of t' (~1e-6 in record units over the 8760 h
+//             span at the base tauT), which moves a far-tail term (|dt'| >= 3.46,
+//             at most 2^-12) by ~2.6e-6 |dt'| relative, with a sign that varies
+//             with the pair.  Self-excitation terms of such a tile pair still
+//             use the full hi + lo difference.
 constexpr int kSpaceLo = 1;
 constexpr int kPolyExp = 2;
+constexpr int kTimeHiOnly = 4;
 
 // Coefficients of p(f) ~ 2^f on [-1/2, 1/2], degree 6, fitted in relative
 // error by hawkes_b200/csrc/fit_exp2.py with sequential FP32 rounding: max
@@ -596,8 +604,21 @@ __device__ __forceinline__ void geometry2(const StagedTile<D>& t, int p, const R
         if (V & kSpaceLo) dd = add2(dd, add2(w.xl[r][k], reinterpret_cast<const float2*>(t.nxl[k])[p]));
         d2 = k == 0 ? mul2(dd, dd) : fma2(dd, dd, d2);
     }
-    dt = add2(add2(w.th[r], reinterpret_cast<const float2*>(t.nt)[p]),
-              add2(w.tl[r], reinterpret_cast<const float2*>(t.ntl)[p]));
+    if (V & kTimeHiOnly)
+        dt = add2(w.th[r], reinterpret_cast<const float2*>(t.nt)[p]);
+    else
+        dt = add2(add2(w.th[r], reinterpret_cast<const float2*>(t.nt)[p]),
+                  add2(w.tl[r], reinterpret_cast<const float2*>(t.ntl)[p]));
+}
+
+// The time difference the self-excitation terms use: hi + lo always, added
+// in the same order as geometry2's full difference.
+template <int D, int R, int V>
+__device__ __forceinline__ float2 self_dt2(const StagedTile<D>& t, int p, const Rows2<D, R>& w,
+                                           int r, float2 dt) {
+    if (V & kTimeHiOnly)
+        return add2(dt, add2(w.tl[r], reinterpret_cast<const float2*>(t.ntl)[p]));
+    return dt;
 }
 
 // Row-order pass over column pairs [p0, p1) of the staged tile (broadcast
@@ -621,10 +642,11 @@ __device__ __forceinline__ void body_f32(const StagedTile<D>& t, int p0, int p1,
                 a[r][2] = fma2(B, t2, a[r][2]);
             }
             if (DO_S) {
-                const float2 S = self_excite2<V, MASK>(d2, dt, w.rk[r], rj, c);
+                const float2 dts = self_dt2<D, R, V>(t, p, w, r, dt);
+                const float2 S = self_excite2<V & ~kTimeHiOnly, MASK>(d2, dts, w.rk[r], rj, c);
                 a[r][3] = add2(a[r][3], S);
                 a[r][4] = fma2(S, d2, a[r][4]);
-                a[r][5] = fma2(S, dt, a[r][5]);
+                a[r][5] = fma2(S, dts, a[r][5]);
             }
         }
     }
@@ -722,10 +744,11 @@ __device__ __forceinline__ void sym_group_f32(const StagedTile<D>& t, int g, int
                 cp[2][m] = fma2(B, t2, cp[2][m]);
             }
             if (DO_S) {
-                const float2 S = self_excite2<V, MASK>(d2, dt, w.rk[r], rj, c);
+                const float2 dts = self_dt2<D, R, V>(t, p, w, r, dt);
+                const float2 S = self_excite2<V & ~kTimeHiOnly, MASK>(d2, dts, w.rk[r], rj, c);
                 a[r][3] = add2(a[r][3], S);
                 a[r][4] = fma2(S, d2, a[r][4]);
-                a[r][5] = fma2(S, dt, a[r][5]);
+                a[r][5] = fma2(S, dts, a[r][5]);
             }
         }
     }
@@ -864,13 +887,14 @@ __device__ __forceinline__ void f32c_item(const float* __restrict__ rec,
         // terms) never changes it.  A far-tail pair has min|dt| > 0: its j
         // events are all earlier than its i events or all later, so it needs
         // no causality mask.
-        constexpr int VF = V & ~kPolyExp;
+        constexpr int VF = V & ~kPolyExp;         // background exponential of far tiles
+        constexpr int VG = V | kTimeHiOnly;        // their geometry: hi parts of the times
         if (sym && m.doB && jt < ts0) {
             // jt < ts0 <= nTiles - 1: a full tile
             if (m.fastB && !m.doS)
-                tile_sym_f32<D, R, V, VF, false, false>(st, w, c, acc, sCol, colAcc, Npad, j0);
+                tile_sym_f32<D, R, VG, VF, false, false>(st, w, c, acc, sCol, colAcc, Npad, j0);
             else if (m.fastB)
-                tile_sym_f32<D, R, V, VF, true, false>(st, w, c, acc, sCol, colAcc, Npad, j0);
+                tile_sym_f32<D, R, VG, VF, true, false>(st, w, c, acc, sCol, colAcc, Npad, j0);
             else if (!m.doS)
                 tile_sym_f32<D, R, V, V, false, false>(st, w, c, acc, sCol, colAcc, Npad, j0);
             else if (m.allCausal)
@@ -879,9 +903,9 @@ __device__ __forceinline__ void f32c_item(const float* __restrict__ rec,
                 tile_sym_f32<D, R, V, V, true, true>(st, w, c, acc, sCol, colAcc, Npad, j0);
         } else if (m.doB) {
             if (m.fastB && !m.doS)
-                tile_f32<D, R, V, VF, true, false, false>(st, nj, w, c, acc);
+                tile_f32<D, R, VG, VF, true, false, false>(st, nj, w, c, acc);
             else if (m.fastB)
-                tile_f32<D, R, V, VF, true, true, false>(st, nj, w, c, acc);
+                tile_f32<D, R, VG, VF, true, true, false>(st, nj, w, c, acc);
             else if (!m.doS)
                 tile_f32<D, R, V, V, true, false, false>(st, nj, w, c, acc);
             else if (m.allCausal)
