@@ -410,7 +410,9 @@ __device__ __forceinline__ void f64_item(const double* __restrict__ rec,
         if (i < N) {
 #pragma unroll
             for (int q = 0; q < kNumAcc; ++q)
-                partials[((size_t)slot * kNumAcc + q) * Npad + i] = acc[r][q];
+                // a self-excitation-only sweep leaves the background rows to
+                // the kept sums: they are neither written nor read
+                if (q >= 3 || !c.noB) partials[((size_t)slot * kNumAcc + q) * Npad + i] = acc[r][q];
         }
     }
 }
@@ -925,7 +927,9 @@ __device__ __forceinline__ void f32c_item(const float* __restrict__ rec,
         if (i < N) {
 #pragma unroll
             for (int q = 0; q < kNumAcc; ++q)
-                partials[((size_t)slot * kNumAcc + q) * Npad + i] = acc[r][q];
+                // a self-excitation-only sweep leaves the background rows to
+                // the kept sums: they are neither written nor read
+                if (q >= 3 || !c.noB) partials[((size_t)slot * kNumAcc + q) * Npad + i] = acc[r][q];
         }
     }
 }
@@ -1085,6 +1089,10 @@ finish_list_kernel(const FinishProblem* __restrict__ problems,
         double s[kNumAcc];
 #pragma unroll
         for (int q = 0; q < kNumAcc; ++q) {
+            if (q < 3 && P.keptB) {
+                s[q] = P.keptB[(size_t)q * N + i];  // unchanged: not written back
+                continue;
+            }
             double acc = 0.0;
             for (int ch = 0; ch < nc; ++ch)
                 acc += P.partials[((size_t)ch * kNumAcc + q) * P.Npad + i];
@@ -1096,12 +1104,8 @@ finish_list_kernel(const FinishProblem* __restrict__ problems,
                 else
                     acc += (double)P.colAcc[(size_t)q * P.Npad + i] * kColInv;
             }
-            if (q < 3 && P.keptB) {
-                s[q] = P.keptB[(size_t)q * N + i];  // unchanged: not written back
-            } else {
-                s[q] = acc * f.accScale[q];
-                if (P.sums) P.sums[(size_t)q * N + i] = s[q];
-            }
+            s[q] = acc * f.accScale[q];
+            if (P.sums) P.sums[(size_t)q * N + i] = s[q];
         }
         event_contributions(f, s, P.times[i], v, P.probs ? P.probs + i : nullptr);
     }
