@@ -292,7 +292,7 @@ int Executor::build_plan(const std::vector<SetView>& sets, const int* setOf, con
         const int nStrips = (N + stripEvents - 1) / stripEvents;
         const int Npad = nStrips * stripEvents;
         const int CT = std::max(1, (nTiles + nChunksTarget - 1) / nChunksTarget);  // tiles a chunk
-        const int maxChunks = (nTiles + CT - 1) / CT;
+        int maxSlots = 1;  // partial-sum slots the widest strip band uses
         pl.maxN = std::max(pl.maxN, N);
         SweepProblem& sp = pl.sp[p];
         sp.c = pair_consts(prm);
@@ -301,8 +301,6 @@ int Executor::build_plan(const std::vector<SetView>& sets, const int* setOf, con
         sp.Npad = Npad;
         sp.tileMin = s.dTileMin;
         sp.tileMax = s.dTileMax;
-        sp.partials = reinterpret_cast<double*>(partOff);  // offset, fixed up later
-        partOff += (size_t)maxChunks * kNumAcc * Npad;
         // a self-excitation-only sweep has no background, so no column sums
         sp.symmetric = (symmetric && !keptB && N <= kMaxSymmetricEvents) ? 1 : 0;
         if (!fp32 && sp.symmetric) {
@@ -431,7 +429,11 @@ int Executor::build_plan(const std::vector<SetView>& sets, const int* setOf, con
                 pl.items.push_back(w);
             }
             pl.stripChunks.push_back(cLast - cFirst);
+            maxSlots = std::max(maxSlots, cLast - cFirst);
         }
+        // partial sums: as many slots per strip as the widest band uses
+        sp.partials = reinterpret_cast<double*>(partOff);  // offset, fixed up later
+        partOff += (size_t)maxSlots * kNumAcc * Npad;
 
         FinishProblem& fp = pl.fp[p];
         fp.partials = nullptr;  // fixed up later
