@@ -133,3 +133,30 @@ def test_multiset_errors():
         with pytest.raises(hb.HawkesError) as ei:
             m.setData(2, np.zeros(400), np.zeros(200))
         assert ei.value.status == 3
+
+
+@pytest.mark.parametrize("flags", [FP64, FP32C], ids=["fp64", "fp32c"])
+def test_multiset_degenerate_sizes_vs_oracle(flags):
+    # single events, block-boundary sizes, tied and unsorted times, each set at
+    # its own parameters, all in one run
+    rng = np.random.default_rng(43)
+    sizes = [1, 2, 3, 31, 127, 128, 129, 300]
+    sets = []
+    for k, n in enumerate(sizes):
+        loc = rng.uniform(0.0, 20.0, size=(n, 2))
+        t = np.sort(rng.uniform(0.0, 8760.0, size=n))
+        if k == 6:
+            t = np.floor(t / 200.0) * 200.0  # ties
+        if k == 7:
+            # unsorted; the last time stays the largest, since the model's
+            # horizon T is the last time given (as in the reference)
+            t = np.append(rng.permutation(t[:-1]), t[-1])
+        p = np.asarray(workloads.BASE_PARAMS) * np.exp(0.3 * rng.standard_normal(6))
+        sets.append((loc, t, p))
+    with hb.Multiset(2, sizes, flags, 0) as m:
+        for s, (loc, t, _) in enumerate(sets):
+            m.setData(s, loc, t)
+        ll, g = m.logLikelihoodAndGradient(np.stack([p for _, _, p in sets]))
+    for s, (loc, t, p) in enumerate(sets):
+        o = oracle.oracle_eval(loc, t, p, threads=4)
+        check_vs_oracle(ll[s], g[s], o, flags, f"set {s} (N={sizes[s]})")
