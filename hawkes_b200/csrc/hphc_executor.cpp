@@ -37,6 +37,71 @@ void tile_needs(double tminI, double tmaxI, double tminJ, double tmaxJ, const Pa
     *doS = (dtHi > 0.0) && !(c.skipS >= 0.0 && allCausal && -c.cW * dtLo >= c.skipS);
 }
 
+// Band [*lo, *hi) of j tiles that strip st (r tiles of targets) must visit:
+// the tiles that may hold a non-zero term for constants c (for sorted times a
+// contiguous range found by bisection on the tile bounds, one tile of margin
+// each side); wide: for any sigma and omega (the device-resident loop).
+void strip_band(const SetView& s, const PairConsts& c, bool symmetric, bool wide, int r,
+                int nTiles, int st, int* loOut, int* hiOut) {
+    const int ts0 = st * r, ts1 = std::min(ts0 + r, nTiles);
+    double tminI = INFINITY, tmaxI = -INFINITY;
+    for (int t = ts0; t < ts1; ++t) {
+        tminI = std::min(tminI, s.hTileMin[t]);
+        tmaxI = std::max(tmaxI, s.hTileMax[t]);
+    }
+    int lo = 0, hi = nTiles;
+    if (s.sorted && wide) {
+        // any sampled sigma, omega: every earlier tile may hold
+        // self-excitation terms; the background band (tauT fixed)
+        // is as below
+        auto neededB = [&](int jt) {
+            bool b, se;
+            tile_needs(tminI, tmaxI, s.hTileMin[jt], s.hTileMax[jt], c, &b, &se);
+            return b;
+        };
+        lo = 0;
+        if (symmetric) {
+            hi = ts1;
+        } else {
+            int a = ts1, b = nTiles;
+            while (a < b) {
+                const int m = (a + b) / 2;
+                if (neededB(m)) a = m + 1; else b = m;
+            }
+            hi = std::min(nTiles, a + 1);
+        }
+    } else if (s.sorted) {
+        auto needed = [&](int jt) {
+            bool b, se;
+            tile_needs(tminI, tmaxI, s.hTileMin[jt], s.hTileMax[jt], c, &b, &se);
+            return b || se;
+        };
+        // left of the strip the test is non-decreasing in jt, right of
+        // it non-increasing (times ascending); keep one tile of margin
+        int a = 0, b = ts0;
+        while (a < b) {
+            const int m = (a + b) / 2;
+            if (needed(m)) b = m; else a = m + 1;
+        }
+        lo = std::max(0, a - 1);
+        if (symmetric) {
+            // pairs with later tiles are added as columns by the later
+            // strips; sorted times leave no self-excitation there
+            hi = ts1;
+        } else {
+            a = ts1;
+            b = nTiles;
+            while (a < b) {
+                const int m = (a + b) / 2;
+                if (needed(m)) a = m + 1; else b = m;
+            }
+            hi = std::min(nTiles, a + 1);
+        }
+    }
+    *loOut = lo;
+    *hiOut = hi;
+}
+
 int f32_stride(int D) {
     return (2 * (D + 1) + 1 + 3) / 4 * 4;
 }
@@ -272,6 +337,38 @@ int Executor::build_plan(const std::vector<SetView>& sets, const int* setOf, con
     const int target = numSMs_ * items * std::max(1, shardWorld);
     const int nChunksTarget = std::max(1, (int)std::ceil(target / std::max(1.0, totalStrips)));
 
+    // A self-excitation-only sweep (kept background sums, host-planned bands)
+    // visits a few tiles near each strip.  With fewer strips than two per
+    // resident CTA (one problem, say), the general grid leaves about one wave
+    // of items, where the few left over double the sweep's time: the bands
+    // are then cut on a grid set from their total, estimated from up to 16
+    // strips a problem, for about four items per resident CTA (never coarser
+    // than the general grid).  With more strips each band stays one item.
+    int selfCT = 0;
+    if (keptB && !wideBands_ && totalStrips < 2.0 * sweep_grid(r)) {
+        double bandTiles = 0.0;
+        for (int p = 0; p < P; ++p) {
+            const SetView& s = sets[setOf[p]];
+            const PairConsts c = pair_consts(params + (size_t)6 * p);
+            const int nTiles = (s.N + kTile - 1) / kTile;
+            const int nStrips = (s.N + stripEvents - 1) / stripEvents;
+            const int step = std::max(1, nStrips / 16);
+            double sampled = 0.0;
+            int n = 0;
+            for (int st = 0; st < nStrips; st += step, ++n) {
+                int lo = 0, hi = nTiles;
+                strip_band(s, c, false, false, r, nTiles, st, &lo, &hi);
+                sampled += hi - lo;
+            }
+            bandTiles += sampled * nStrips / std::max(1, n);
+        }
+        // a power of two near it, so that small changes of the bands (a
+        // sampler's steps in omega) keep the grid, the list's capacity and
+        // the captured graph
+        const double want = std::max(1.0, bandTiles / (4.0 * sweep_grid(r)));
+        selfCT = 1 << (int)std::lround(std::log2(want));
+    }
+
     size_t recOff = 0, partOff = 0, colOff = 0;
     std::vector<size_t> chunkBase(P);
     int blockBase = 0;
@@ -291,7 +388,10 @@ int Executor::build_plan(const std::vector<SetView>& sets, const int* setOf, con
         const int nTiles = (N + kTile - 1) / kTile;
         const int nStrips = (N + stripEvents - 1) / stripEvents;
         const int Npad = nStrips * stripEvents;
-        const int CT = std::max(1, (nTiles + nChunksTarget - 1) / nChunksTarget);  // tiles a chunk
+        // tiles a chunk (a self-excitation-only grid never coarser than the
+        // general one, which follows the tuned items per SM)
+        const int generalCT = std::max(1, (nTiles + nChunksTarget - 1) / nChunksTarget);
+        const int CT = selfCT > 0 ? std::min(selfCT, generalCT) : generalCT;
         int maxSlots = 1;  // partial-sum slots the widest strip band uses
         pl.maxN = std::max(pl.maxN, N);
         SweepProblem& sp = pl.sp[p];
@@ -358,61 +458,8 @@ int Executor::build_plan(const std::vector<SetView>& sets, const int* setOf, con
         // work items: each strip's band of tiles that may hold a non-zero term
         chunkBase[p] = pl.stripChunks.size();
         for (int st = 0; st < nStrips; ++st) {
-            const int ts0 = st * r, ts1 = std::min(ts0 + r, nTiles);
-            double tminI = INFINITY, tmaxI = -INFINITY;
-            for (int t = ts0; t < ts1; ++t) {
-                tminI = std::min(tminI, s.hTileMin[t]);
-                tmaxI = std::max(tmaxI, s.hTileMax[t]);
-            }
             int lo = 0, hi = nTiles;
-            if (s.sorted && wideBands_) {
-                // any sampled sigma, omega: every earlier tile may hold
-                // self-excitation terms; the background band (tauT fixed)
-                // is as below
-                auto neededB = [&](int jt) {
-                    bool b, se;
-                    tile_needs(tminI, tmaxI, s.hTileMin[jt], s.hTileMax[jt], sp.c, &b, &se);
-                    return b;
-                };
-                lo = 0;
-                if (sp.symmetric) {
-                    hi = ts1;
-                } else {
-                    int a = ts1, b = nTiles;
-                    while (a < b) {
-                        const int m = (a + b) / 2;
-                        if (neededB(m)) a = m + 1; else b = m;
-                    }
-                    hi = std::min(nTiles, a + 1);
-                }
-            } else if (s.sorted) {
-                auto needed = [&](int jt) {
-                    bool b, se;
-                    tile_needs(tminI, tmaxI, s.hTileMin[jt], s.hTileMax[jt], sp.c, &b, &se);
-                    return b || se;
-                };
-                // left of the strip the test is non-decreasing in jt, right of
-                // it non-increasing (times ascending); keep one tile of margin
-                int a = 0, b = ts0;
-                while (a < b) {
-                    const int m = (a + b) / 2;
-                    if (needed(m)) b = m; else a = m + 1;
-                }
-                lo = std::max(0, a - 1);
-                if (sp.symmetric) {
-                    // pairs with later tiles are added as columns by the later
-                    // strips; sorted times leave no self-excitation there
-                    hi = ts1;
-                } else {
-                    a = ts1;
-                    b = nTiles;
-                    while (a < b) {
-                        const int m = (a + b) / 2;
-                        if (needed(m)) a = m + 1; else b = m;
-                    }
-                    hi = std::min(nTiles, a + 1);
-                }
-            }
+            strip_band(s, sp.c, sp.symmetric != 0, wideBands_, r, nTiles, st, &lo, &hi);
             // Chunks sit on a fixed grid of CT tiles per problem, so a tile
             // always lands in the same chunk whatever the band: skipping a
             // band's outside only drops chunks whose sums are exactly zero,
