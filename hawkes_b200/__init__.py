@@ -10,12 +10,13 @@ from .engine import (  # noqa: F401
     PATH_SWEEP,
     PRECISION_FP32_COMP, PRECISION_FP64, SSE, TBB, CudaHawkes, Engine, HawkesError, Multiset,
     createEngine, engineInitial, factory, getGradient, getLogLikelihood, getProbsSelfExcite,
-    setParameters, setTimesData, updateLocations)
+    setParameters, setTimesData, timeTest, updateLocations)
 from .sampler import Potential, Sampler, log_prior, sampler  # noqa: F401
 
 __all__ = [
     "CudaHawkes", "Engine", "HawkesError", "Multiset", "factory", "createEngine", "engineInitial",
     "updateLocations", "setTimesData", "setParameters", "getLogLikelihood",
-    "getProbsSelfExcite", "getGradient", "PARAMETER_NAMES", "Sampler", "sampler", "Potential",
+    "getProbsSelfExcite", "getGradient", "timeTest", "PARAMETER_NAMES", "Sampler", "sampler",
+    "Potential",
     "log_prior",
 ]

@@ -25,6 +25,7 @@ engine's message.
 from __future__ import annotations
 
 import ctypes
+import time
 from typing import Optional
 
 import numpy as np
@@ -479,3 +480,38 @@ def engineInitial(locations, N: int, P: int, times, parameters, threads: int = 0
     engine = setTimesData(engine, times)
     engine = setParameters(engine, parameters)
     return engine
+
+
+def timeTest(locationCount: int = 5000, maxIts: int = 1, threads: int = 0, simd: int = 0,
+             gpu: int = 1, single: int = 0, r: bool = False, seed: int = 666) -> float:
+    """``timeTest()`` (R/Untitled.R:132-175): seconds taken by ``maxIts``
+    log-likelihood evaluations of a random problem in two dimensions
+    (standard normal locations, times 1..N, parameters drawn from Exp(1)),
+    with numpy's generator seeded by ``seed`` in place of R's.
+
+    Every evaluation is the full computation, as the reference recomputes
+    each time: the engine is made with ``NO_INCREMENTAL`` so that repeated
+    calls at unchanged parameters do not reuse kept sums.  ``r=True`` (the
+    naive R implementation) is not part of this package; ``threads`` and
+    ``simd`` are accepted for signature compatibility.
+    """
+    if r:
+        raise HawkesError(5, "timeTest: the naive R implementation is not part of this package")
+    if gpu <= 0:
+        raise HawkesError(5, "timeTest: the CUDA engine needs gpu > 0")
+    rng = np.random.default_rng(seed)
+    n = int(locationCount)
+    locations = rng.standard_normal((n, 2))
+    times = np.arange(1, n + 1, dtype=np.float64)
+    params = rng.exponential(1.0, size=6)
+    flags = OPENCL | CUDA | NO_INCREMENTAL | (FLOAT if single else 0)
+    with CudaHawkes(2, n, flags, gpu) as eng:
+        eng.updateLocations(-1, locations)
+        eng.setTimesData(times)
+        eng.setParameters(params)
+        t0 = time.perf_counter()
+        for _ in range(int(maxIts)):
+            eng.getSumOfLikContribs()
+        elapsed = time.perf_counter() - t0
+    print(f"{elapsed:.6f}")
+    return elapsed

@@ -265,3 +265,14 @@ def test_r_mirror_call_sequence():
     assert np.max(np.abs(hb.getProbsSelfExcite(eng) - o["probs"])) <= 1e-10
     g = hb.getGradient(eng)
     assert np.all(np.abs(g - o["grad"]) <= 1e-10 * o["grad_scale"])
+
+
+def test_r_time_test():
+    # timeTest() (R/Untitled.R:132-175): elapsed seconds of full evaluations
+    s = hb.timeTest(locationCount=2000, maxIts=3, gpu=1)
+    assert 0.0 < s < 60.0
+    assert 0.0 < hb.timeTest(locationCount=1000, maxIts=2, gpu=1, single=1) < 60.0
+    with pytest.raises(hb.HawkesError):
+        hb.timeTest(locationCount=100, r=True)
+    with pytest.raises(hb.HawkesError):
+        hb.timeTest(locationCount=100, gpu=0)
