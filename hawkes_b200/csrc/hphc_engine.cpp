@@ -688,6 +688,11 @@ struct hphc_multiset {
     std::vector<EventSet> sets;
     std::vector<HostBuf<double>> hLoc;
     std::vector<char> ready, dirty;
+    // Each set is uploaded as soon as its data arrives (the copy from its
+    // pinned mirror overlaps the host work on the next sets); its event marks
+    // the end of that copy, which a later setData of the set waits for
+    // before it overwrites the mirror.
+    std::vector<cudaEvent_t> uploaded;
     std::vector<double> hOut;
     int lastLaunches = 0;
 
@@ -701,10 +706,12 @@ struct hphc_multiset {
         hLoc.resize(S);
         ready.assign(S, 0);
         dirty.assign(S, 1);
+        uploaded.assign(S, nullptr);
         for (int s = 0; s < S; ++s) {
             cudaError_t e;
             if ((e = sets[s].alloc(D, sizes[s], rt.mode.precision)) ||
-                (e = hLoc[s].reserve((size_t)sizes[s] * D)))
+                (e = hLoc[s].reserve((size_t)sizes[s] * D)) ||
+                (e = cudaEventCreateWithFlags(&uploaded[s], cudaEventDisableTiming)))
                 return cuda_status(lastError, e, "allocation");
             sets[s].derive_times();
         }
@@ -712,8 +719,10 @@ struct hphc_multiset {
     }
 
     void destroy() {
-        rt.release();
+        rt.release();  // waits for the stream: no copy still reads the mirrors
         DeviceGuard g(rt.device);
+        for (auto& ev : uploaded)
+            if (ev) cudaEventDestroy(ev);
         for (auto& s : sets) s.release();
         for (auto& h : hLoc) h.release();
     }
@@ -1186,11 +1195,21 @@ int hphc_multiset_set_data(hphc_multiset* m, int set, const double* locations, s
     size_t bad = 0;
     if (!all_finite(locations, locLength, &bad) || !all_finite(times, timesLength, &bad))
         return fmt(m->lastError, HPHC_ERR_NONFINITE, "set %d: non-finite input", set);
+    DeviceGuard g(m->rt.device);
+    if (!g.ok) return fmt(m->lastError, HPHC_ERR_CUDA, "cannot select device %d", m->rt.device);
+    cudaError_t e = cudaEventSynchronize(m->uploaded[set]);  // the last copy from the mirror
+    if (e != cudaSuccess) return cuda_status(m->lastError, e, "wait for the set's upload");
     std::memcpy(m->hLoc[set].p, locations, locLength * sizeof(double));
     std::memcpy(es.hTimes.p, times, timesLength * sizeof(double));
     es.derive_times();
     m->ready[set] = 1;
     m->dirty[set] = 1;
+    // upload now, overlapping the host work on the next sets
+    int launches = 0;
+    if ((e = es.upload(m->hLoc[set].p, m->rt.mode.precision, m->rt.stream, &launches)) ||
+        (e = cudaEventRecord(m->uploaded[set], m->rt.stream)))
+        return cuda_status(m->lastError, e, "upload");
+    m->dirty[set] = 0;
     return HPHC_OK;
 }
 
