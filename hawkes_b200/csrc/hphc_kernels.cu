@@ -131,7 +131,16 @@ __device__ __forceinline__ TileMode tile_mode(double tminI, double tmaxI, double
 
 // ----------------------------------------------------------- FP64 sweep --
 
-template <int D, int R, bool DO_B, bool DO_S, bool MASK>
+// FP64 background term exp(x): CUDA's exp(), or for far-tail tile pairs
+// (every term at most 2^-60, see kFastTailLog2F64) the FP32 hardware
+// exponential.
+template <bool FAST>
+__device__ __forceinline__ double background_f64(double x) {
+    if (FAST) return (double)ex2_ftz((float)(x * 1.44269504088896340735992468100189214));
+    return exp(x);
+}
+
+template <int D, int R, bool DO_B, bool DO_S, bool MASK, bool FAST = false>
 __device__ __forceinline__ void body_f64(const double* __restrict__ sRec, int nj,
                                          const double (&xi)[R][D], const double (&ti)[R],
                                          const PairConsts& c, double (&acc)[R][kNumAcc]) {
@@ -156,7 +165,7 @@ __device__ __forceinline__ void body_f64(const double* __restrict__ sRec, int nj
             const double dt = ti[r] - rj[D];
             if (DO_B) {
                 const double t2 = dt * dt;
-                const double B = exp(fma(c.cA, d2, c.cB * t2));
+                const double B = background_f64<FAST>(fma(c.cA, d2, c.cB * t2));
                 acc[r][0] += B;
                 acc[r][1] = fma(B, d2, acc[r][1]);
                 acc[r][2] = fma(B, t2, acc[r][2]);
@@ -199,7 +208,7 @@ __device__ __forceinline__ void add_fixed2(unsigned long long* hi, unsigned long
     atomicAdd(lo, (unsigned long long)rint(ldexp(scaled - whole, kColLoBits)));
 }
 
-template <int D, int R, bool DO_S, bool MASK>
+template <int D, int R, bool DO_S, bool MASK, bool FAST = false>
 __device__ __forceinline__ void tile_sym_f64(const double* __restrict__ sRec,
                                              const double (&xi)[R][D], const double (&ti)[R],
                                              const PairConsts& c, double (&acc)[R][kNumAcc],
@@ -234,7 +243,7 @@ __device__ __forceinline__ void tile_sym_f64(const double* __restrict__ sRec,
                 }
                 const double dt = ti[r] - rj[D];
                 const double t2 = dt * dt;
-                const double B = exp(fma(c.cA, d2, c.cB * t2));
+                const double B = background_f64<FAST>(fma(c.cA, d2, c.cB * t2));
                 const double Bd = B * d2, Bt = B * t2;
                 acc[r][0] += B;
                 acc[r][1] += Bd;
@@ -379,7 +388,22 @@ __device__ __forceinline__ void f64_item(const double* __restrict__ rec,
         double2* dst = reinterpret_cast<double2*>(sRec);
         for (int v = tid; v < nj * (S / 2); v += kSweepThreads) dst[v] = src[v];
         __syncthreads();
-        if (sym && m.doB && jt < ts0) {
+        // Far-tail tile pairs (every background term at most 2^-60) take them
+        // from the FP32 hardware exponential; the choice depends on the
+        // background bound alone, and such a pair needs no causality mask.
+        if (sym && m.doB && jt < ts0 && m.fastB) {
+            if (!m.doS)
+                tile_sym_f64<D, R, false, false, true>(sRec, xi, ti, c, acc, sCol, colAcc, Npad,
+                                                       j0, shift);
+            else
+                tile_sym_f64<D, R, true, false, true>(sRec, xi, ti, c, acc, sCol, colAcc, Npad,
+                                                      j0, shift);
+        } else if (m.doB && m.fastB && !(sym && jt < ts0)) {
+            if (!m.doS)
+                body_f64<D, R, true, false, false, true>(sRec, nj, xi, ti, c, acc);
+            else
+                body_f64<D, R, true, true, false, true>(sRec, nj, xi, ti, c, acc);
+        } else if (sym && m.doB && jt < ts0) {
             // jt < ts0 <= nTiles - 1: a full tile
             if (!m.doS)
                 tile_sym_f64<D, R, false, false>(sRec, xi, ti, c, acc, sCol, colAcc, Npad, j0,

@@ -47,9 +47,10 @@ struct PairConsts {
     // in it is exactly zero in the working precision: cA <= 0, cB < 0 and
     // -cB * min|dt|^2 >= skipB.  Likewise for S with -cW * min(dt) >= skipS.
     double skipB, skipS;                   // natural-log thresholds; < 0 disables
-    // FP32 mode: a tile pair whose background terms are all below
-    // exp(-fastB) (natural log; < 0 disables) takes them from the hardware
-    // exponential (see kFastTailLog2).
+    // A tile pair whose background terms are all below exp(-fastB) (natural
+    // log; <= 0 disables) takes them from the hardware ex2.approx: instead of
+    // the polynomial in the FP32 mode (2^-12, kFastTailLog2), of CUDA's exp()
+    // in the FP64 mode (2^-60, kFastTailLog2F64).
     double fastB;
     // Self-excitation-only sweep: no background term is evaluated (the
     // finish takes the background sums from an earlier sweep, which depend
@@ -80,7 +81,8 @@ struct ConstsSpec {
     int variant;      // FP32 variant bits (2 = software exponential)
     int skip;         // tile-level underflow skip on
     double ex2Bias;   // mean relative error of ex2.approx (hardware-exponential variant)
-    int fastTail;     // FP32 software-exponential variant: far tile pairs use the hardware one
+    int fastTail;     // far-tail tile pairs use the hardware exponential (FP32 software-
+                      // exponential variant, and FP64)
     int noB;          // self-excitation-only sweep (PairConsts::noB)
 };
 
@@ -92,6 +94,13 @@ struct ConstsSpec {
 // event's unit sums even weighted by dt'^2, and the hardware exponential's
 // relative error (< 1e-7) moves those sums by under ~5e-11.
 constexpr double kFastTailLog2 = 12.0;
+
+// FP64 mode: a tile pair whose background terms are all at most 2^-60 takes
+// them from the FP32 hardware exponential (relative error ~1e-7; zero below
+// 2^-126).  All such terms of one event add up to at most N 2^-60 of its own
+// term, so their error moves its sums by under N * 1e-25: below FP64
+// rounding for any N this engine holds.
+constexpr double kFastTailLog2F64 = 60.0;
 
 // Underflow thresholds (natural-log units) for the tile-pair skip.  FP32:
 // both exponentials return +0 for any argument below -126.5 (log2 units); a
@@ -134,8 +143,8 @@ inline void param_consts(const double* p, const ConstsSpec& s, PairConsts& c, Fi
     c.skipB = (s.skip && c.cB < 0.0 && c.cA <= 0.0) ? thr : -1.0;
     c.skipS = (s.skip && c.cW < 0.0 && c.cS <= 0.0) ? thr : -1.0;
     const double kLn2 = 0.693147180559945309417232121458176568;
-    c.fastB = (fp32 && s.fastTail && (s.variant & 2) && c.cB < 0.0 && c.cA <= 0.0)
-                  ? kFastTailLog2 * kLn2
+    c.fastB = (s.fastTail && (!fp32 || (s.variant & 2)) && c.cB < 0.0 && c.cA <= 0.0)
+                  ? (fp32 ? kFastTailLog2 : kFastTailLog2F64) * kLn2
                   : -1.0;
     c.noB = s.noB;
     c.pad = 0;

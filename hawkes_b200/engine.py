@@ -50,7 +50,7 @@ FP32_SPACE_HILO = 1 << 12
 ORDERED = 1 << 13       # both orders of every background pair, either precision
 FP32_ORDERED = ORDERED  # earlier name of the same bit
 NO_INCREMENTAL = 1 << 14
-NO_FAST_TAIL = 1 << 15  # FP32-compensated: polynomial exponential for the far tail too
+NO_FAST_TAIL = 1 << 15  # one exponential for every term, the far tail included
 
 # Fault-injection stages (CudaHawkes.injectFault).
 FAULT_UPLOAD = 1

@@ -78,11 +78,11 @@ extern "C" {
                                                 an evaluation at unchanged parameters after
                                                 a few single-event updateLocations calls
                                                 updates the kept per-event sums in O(N)) */
-#define HPHC_FLAG_NO_FAST_TAIL (1L << 15)    /* FP32-compensated mode: the polynomial
-                                                exponential for every pair term (by default
-                                                tile pairs whose background terms are all
-                                                below 2^-12 of an event's own term take those
-                                                terms from ex2.approx) */
+#define HPHC_FLAG_NO_FAST_TAIL (1L << 15)    /* one exponential for every pair term (by
+                                                default tile pairs whose background terms are
+                                                all below 2^-12 (FP32-compensated mode) or
+                                                2^-60 (FP64 mode) of an event's own term take
+                                                those terms from ex2.approx) */
 
 /* How the last evaluation was computed (hphc_get_last_evaluation_path). */
 #define HPHC_PATH_SWEEP 0        /* the O(N^2) pair sweep                             */
