@@ -38,65 +38,55 @@ void tile_needs(double tminI, double tmaxI, double tminJ, double tmaxJ, const Pa
 }
 
 // Band [*lo, *hi) of j tiles that strip st (r tiles of targets) must visit:
-// the tiles that may hold a non-zero term for constants c (for sorted times a
-// contiguous range found by bisection on the tile bounds, one tile of margin
-// each side); wide: for any sigma and omega (the device-resident loop).
+// every tile that may hold a non-zero term for constants c, plus one tile of
+// margin each side; wide: for any sigma and omega (the device-resident
+// loop).  For sorted times the tile bounds are non-decreasing, and a tile
+// before the strip can hold a background term only if its time gap is below
+// dB = sqrt(skipB / -cB), a self-excitation term only below
+// dS = skipS / -cW (tile_mode's underflow tests solved for the gap), so each
+// edge is one binary search on the bounds.  The band may keep a few tiles
+// those tests would drop (tile_mode also tests causality and the space
+// coefficient); the sweep decides every tile itself, and chunks sit on a
+// fixed grid, so a wider band never changes a bit of the result.
 void strip_band(const SetView& s, const PairConsts& c, bool symmetric, bool wide, int r,
                 int nTiles, int st, int* loOut, int* hiOut) {
     const int ts0 = st * r, ts1 = std::min(ts0 + r, nTiles);
-    double tminI = INFINITY, tmaxI = -INFINITY;
-    for (int t = ts0; t < ts1; ++t) {
-        tminI = std::min(tminI, s.hTileMin[t]);
-        tmaxI = std::max(tmaxI, s.hTileMax[t]);
+    *loOut = 0;
+    *hiOut = nTiles;
+    if (!s.sorted) return;
+    const double tminI = s.hTileMin[ts0], tmaxI = s.hTileMax[ts1 - 1];
+    // gap beyond which every term of the kind is exactly zero (+inf: none)
+    const double kInf = INFINITY;
+    const bool anyB = !c.noB;
+    const double dB = !anyB ? -kInf
+                    : (c.skipB >= 0.0 && c.cB < 0.0 && c.cA <= 0.0) ? std::sqrt(c.skipB / -c.cB)
+                                                                      : kInf;
+    const double dS = (c.skipS >= 0.0 && c.cW < 0.0 && c.cS <= 0.0) ? c.skipS / -c.cW : kInf;
+    // left edge: the first tile before the strip whose gap tminI - tmaxJ is
+    // below the larger distance (wide: any sigma, omega, so every tile)
+    int lo = 0;
+    if (!wide) {
+        const double d = std::max(dB, dS);
+        if (d < kInf) {
+            const double* first = std::upper_bound(s.hTileMax, s.hTileMax + ts0, tminI - d);
+            lo = std::max(0, (int)(first - s.hTileMax) - 1);
+        }
     }
-    int lo = 0, hi = nTiles;
-    if (s.sorted && wide) {
-        // any sampled sigma, omega: every earlier tile may hold
-        // self-excitation terms; the background band (tauT fixed)
-        // is as below
-        auto neededB = [&](int jt) {
-            bool b, se;
-            tile_needs(tminI, tmaxI, s.hTileMin[jt], s.hTileMax[jt], c, &b, &se);
-            return b;
-        };
-        lo = 0;
-        if (symmetric) {
-            hi = ts1;
+    // right edge: with the symmetric sweep, later tiles add this strip's
+    // pairs as columns (and sorted times leave no self-excitation there);
+    // otherwise the first tile after the strip whose gap tminJ - tmaxI is at
+    // least dB (background only: no causal pair lies after the strip)
+    int hi = ts1;
+    if (!symmetric && ts1 < nTiles && dB > -kInf) {
+        if (dB == kInf) {
+            hi = nTiles;
         } else {
-            int a = ts1, b = nTiles;
-            while (a < b) {
-                const int m = (a + b) / 2;
-                if (neededB(m)) a = m + 1; else b = m;
-            }
-            hi = std::min(nTiles, a + 1);
+            const double* first = std::lower_bound(s.hTileMin + ts1, s.hTileMin + nTiles,
+                                                   tmaxI + dB);
+            hi = std::min(nTiles, (int)(first - s.hTileMin) + 1);
         }
-    } else if (s.sorted) {
-        auto needed = [&](int jt) {
-            bool b, se;
-            tile_needs(tminI, tmaxI, s.hTileMin[jt], s.hTileMax[jt], c, &b, &se);
-            return b || se;
-        };
-        // left of the strip the test is non-decreasing in jt, right of
-        // it non-increasing (times ascending); keep one tile of margin
-        int a = 0, b = ts0;
-        while (a < b) {
-            const int m = (a + b) / 2;
-            if (needed(m)) b = m; else a = m + 1;
-        }
-        lo = std::max(0, a - 1);
-        if (symmetric) {
-            // pairs with later tiles are added as columns by the later
-            // strips; sorted times leave no self-excitation there
-            hi = ts1;
-        } else {
-            a = ts1;
-            b = nTiles;
-            while (a < b) {
-                const int m = (a + b) / 2;
-                if (needed(m)) a = m + 1; else b = m;
-            }
-            hi = std::min(nTiles, a + 1);
-        }
+    } else if (!symmetric && ts1 < nTiles) {
+        hi = std::min(nTiles, ts1 + 1);
     }
     *loOut = lo;
     *hiOut = hi;
