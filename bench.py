@@ -668,6 +668,55 @@ def shard_arm(args):
     return 0
 
 
+def sampler_arm(args):
+    """--workload sampler: iterations per second of the reference's MCMC
+    sampler (R/Untitled.R:254-422) over 16 chains on the headline events
+    (N = 100,000), chains at the base parameters with tauX and tauT fixed as
+    the reference keeps them: the host driver, the graph-replayed device
+    driver, and the host driver on an engine that keeps no sums (every
+    iteration a full sweep of every chain).  One process, one GPU."""
+    import torch
+
+    import hawkes_b200 as hb
+
+    w = make_workload("headline", args.n)
+    loc, t, base = w["loc"], w["t"], w["params"]
+    K = 16
+    its = max(3, args.steps // 10)
+    init = np.tile(base, (K, 1))
+    arms = {}
+    with ClockSampler() as clocks:
+        for name, flags, device in (("host", hb.CUDA | hb.COMPENSATED, False),
+                                    ("device", hb.CUDA | hb.COMPENSATED, True),
+                                    ("host_no_reuse",
+                                     hb.CUDA | hb.COMPENSATED | hb.NO_INCREMENTAL, False)):
+            with hb.CudaHawkes(2, len(t), flags, 0) as e:
+                e.setTimesData(t)
+                e.updateLocations(-1, loc)
+                e.setParameters(base)
+                with hb.Sampler(init, radius=0.3, seed=SEED) as s:
+                    s.run(e, args.warmup, device=device)
+                    n = its if name != "host_no_reuse" else max(3, its // 10)
+                    torch.cuda.synchronize()
+                    t0 = time.perf_counter()
+                    s.run(e, n, device=device)
+                    torch.cuda.synchronize()
+                    arms[name] = (time.perf_counter() - t0) / n
+    out = {
+        "metric": f"sampler iterations/s, {K} chains, N={args.n} (FP32-compensated)",
+        "value": 1.0 / arms["device"], "unit": "iterations/s", "n_gpus": 1, "steps": its,
+        "warmup": args.warmup, "ms_per_step": 1e3 * arms["device"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "data": "synthetic",
+        "dtype": "f32 pair terms (compensated), f64 reductions",
+        "config": {"workload": w["desc"] + f"; {K} chains at the base parameters, random-scan "
+                   "proposals of sigma, omega, theta, mu0 (radius 0.3)", "chains": K},
+        "ms_per_iteration": {k: 1e3 * v for k, v in arms.items()},
+        "clocks": clocks.summary(None),
+    }
+    print(json.dumps(out))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -676,7 +725,7 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--n", type=int, default=N_EVENTS, help=argparse.SUPPRESS)
     ap.add_argument("--workload", default="headline",
-                    choices=("headline", "batched", "uneven", "clustered"),
+                    choices=("headline", "batched", "uneven", "clustered", "sampler"),
                     help="headline (default): the metric's N=100k workload; the others are "
                          "the batched-proposal, uneven-set and clustered configurations")
     ap.add_argument("--steps64", type=int, default=0,
@@ -693,6 +742,8 @@ def main():
         return reference_arm(args)
     if args.shard:
         return shard_arm(args)
+    if args.workload == "sampler":
+        return sampler_arm(args)
     return ours_arm(args)
 
 
