@@ -524,8 +524,11 @@ def ours_arm(args):
         "terms": {"background": nb, "self_excitation": ns, "possible": 2 * pairs,
                   "background_exponentials": nev,
                   "note": "pair terms the sweep accounted for; the rest are the non-causal half "
-                          "of the self-excitation sum and tile pairs whose terms are all exactly "
-                          "zero in FP32.  A background pair with the other event in an earlier "
+                          "of the self-excitation sum, self-excitation tile pairs whose terms "
+                          "are all exactly zero in FP32, and background tile pairs whose terms "
+                          "are all below 2^-91 of an event's own term (tail truncation: under "
+                          "2^-60 of any event's sums).  A background pair with the other event "
+                          "in an earlier "
                           "tile is evaluated once (one exponential) for both events"},
         "roofline": {"bound": "fp32", "kernel": kernel,
                      "achieved": achieved, "peak": peak_inst, "unit": "Tinst/s",

@@ -5,7 +5,8 @@ the C ABI in include/hphc.h); this package is its Python host interface.
 """
 from .engine import (  # noqa: F401
     AVX, AVX512, COMPENSATED, CUDA, FLOAT, FP32_FAST_EXP, FP32_ORDERED, FP32_SPACE_HILO, ORDERED,
-    FAULT_LAUNCH, FAULT_UPLOAD, FAULT_WAIT, NO_FAST_TAIL, NO_INCREMENTAL, NO_UNDERFLOW_SKIP,
+    FAULT_LAUNCH, FAULT_UPLOAD, FAULT_WAIT, NO_FAST_TAIL, NO_INCREMENTAL, NO_TAIL_TRUNCATION,
+    NO_UNDERFLOW_SKIP,
     OPENCL, PARAMETER_NAMES, PATH_INCREMENTAL, PATH_KEPT_SUMS, PATH_SELF_EXCITATION,
     PATH_SWEEP,
     PRECISION_FP32_COMP, PRECISION_FP64, SSE, TBB, CudaHawkes, Engine, HawkesError, Multiset,

@@ -143,6 +143,7 @@ struct Mode {
     bool underflowSkip = true;
     bool symmetric = true;  // each background pair evaluated once for both events
     bool fastTail = true;   // far-tail background tile pairs on the hardware exponential
+    bool truncateTail = true;  // background tile pairs below 2^-91 of B_ii skipped
 };
 
 Mode mode_from_flags(long fl) {
@@ -154,6 +155,7 @@ Mode mode_from_flags(long fl) {
                 ((fl & HPHC_FLAG_FP32_FAST_EXP) ? 0 : 2);
     m.symmetric = !(fl & HPHC_FLAG_ORDERED);
     m.fastTail = !(fl & HPHC_FLAG_NO_FAST_TAIL);
+    m.truncateTail = !(fl & HPHC_FLAG_NO_TAIL_TRUNCATION);
     return m;
 }
 
@@ -325,6 +327,7 @@ struct Runtime {
                                ex2Bias);
         ex.symmetric = mode.symmetric;
         ex.fastTail = mode.fastTail;
+        ex.truncateTail = mode.truncateTail;
         if (st) err = ex.error;
         return st;
     }

@@ -272,6 +272,7 @@ ConstsSpec Executor::consts_spec() const {
     s.D = D_;
     s.variant = variant_;
     s.skip = skip_ ? 1 : 0;
+    s.truncate = (skip_ && truncateTail) ? 1 : 0;
     s.ex2Bias = ex2Bias_;
     s.fastTail = fastTail ? 1 : 0;
     s.noB = keptB ? 1 : 0;
@@ -673,7 +674,8 @@ int Executor::autotune(const std::vector<SetView>& sets, const int* setOf, const
     double pairs = 0.0;
     for (int p = 0; p < P; ++p) pairs += (double)sets[setOf[p]].N * sets[setOf[p]].N;
     pairs /= std::max(1, shardWorld);  // work of this rank
-    const int mode = variant_ | (symmetric ? 16 : 0) | (fastTail ? 32 : 0) | (skip_ ? 64 : 0);
+    const int mode = variant_ | (symmetric ? 16 : 0) | (fastTail ? 32 : 0) | (skip_ ? 64 : 0) |
+                     (truncateTail ? 128 : 0);
     const TuneKey key = std::make_tuple(D_, precision_, mode, log2_bucket(pairs), log2_bucket(P));
     if (deviceName_.empty()) {
         cudaDeviceProp prop{};

@@ -95,6 +95,7 @@ public:
     bool kernelTiming = false;
     bool symmetric = false;  // symmetric background sweep (set before the first enqueue)
     bool fastTail = true;    // FP32 polynomial mode: far-tail tile pairs use ex2.approx
+    bool truncateTail = true;  // skip background tile pairs below 2^-91 of B_ii (with the skip)
     // Sharded sweep: with shardWorld > 1 the plan keeps only the target
     // strips assigned to shardRank (whole strips, balanced by their tile
     // counts; every rank computes the same assignment), and the finish takes

@@ -8,10 +8,12 @@
 // j tiles; each kTile-event j tile is staged in shared memory with coalesced
 // 16-byte loads and read back as broadcasts.  Per (strip, tile) the CTA
 // decides from FP64 time bounds whether the tile pair has any background term
-// above the underflow threshold, any causal (t_j < t_i) self-excitation term,
+// above the skip threshold, any causal (t_j < t_i) self-excitation term,
 // and whether the causal mask is needed, so the non-causal half of the
-// self-excitation sum is skipped at tile level.  Skipped terms are exactly zero
-// in the working precision, so skipping does not change any bit of the result.
+// self-excitation sum is skipped at tile level.  Skipped self-excitation terms
+// are exactly zero in the working precision; skipped background terms are
+// zero too, or with tail truncation (the default) each at most 2^-91 of the
+// event's own background term, which moves its sums by under 2^-60.
 //
 // All sums are written per (chunk, event) and combined in chunk order, then
 // reduced over events with fixed shuffle trees: results do not depend on

@@ -43,9 +43,10 @@ struct PairConsts {
     // S exponent (log2 units) = kS |dx'|^2 + kW dt' with kS = -sigma^2 / a^2 and
     // kW = -omega log2(e) / sT, each split hi + lo.
     float fSh, fSl, fWh, fWl;
-    // Tile-pair underflow skips.  A tile pair is skipped for B when every B_u
-    // in it is exactly zero in the working precision: cA <= 0, cB < 0 and
-    // -cB * min|dt|^2 >= skipB.  Likewise for S with -cW * min(dt) >= skipS.
+    // Tile-pair skips.  A tile pair is skipped for B when cA <= 0, cB < 0 and
+    // -cB * min|dt|^2 >= skipB: every B_u in it is exactly zero in the working
+    // precision, or (tail truncation) at most 2^-kNegligibleLog2.  S is
+    // skipped only where every S_u underflows: -cW * min(dt) >= skipS.
     double skipB, skipS;                   // natural-log thresholds; < 0 disables
     // A tile pair whose background terms are all below exp(-fastB) (natural
     // log; <= 0 disables) takes them from the hardware ex2.approx: instead of
@@ -80,6 +81,7 @@ struct ConstsSpec {
     int D;
     int variant;      // FP32 variant bits (2 = software exponential)
     int skip;         // tile-level underflow skip on
+    int truncate;     // background tail truncation at 2^-kNegligibleLog2 (needs skip)
     double ex2Bias;   // mean relative error of ex2.approx (hardware-exponential variant)
     int fastTail;     // far-tail tile pairs use the hardware exponential (FP32 software-
                       // exponential variant, and FP64)
@@ -110,6 +112,18 @@ constexpr double kFastTailLog2F64 = 60.0;
 constexpr double kSkipF32 = 88.0;
 constexpr double kSkipF64 = 760.0;
 
+// Background tail truncation.  Every event's background sum holds its own
+// term, B_ii = 1 unit, the largest of all its terms.  A tile pair whose
+// background terms are all at most 2^-91 units is skipped: the skipped
+// terms of one event add up to at most N 2^-91 <= 2^-60 of its sum (N <
+// 2^31), and those weighted by a squared scaled distance x (the gradient
+// sums) to at most x e^-x <= 64 2^-91 each, since x >= 91 ln 2 there.  That
+// is below FP64 rounding of the sums in both modes.  At b = 1/336 per hour
+// the cut falls at |dt| = 11.2 / b = 3774 h, against 13.3 / b for FP32
+// underflow.  The self-excitation sums have no such lower bound and keep the
+// underflow skip only.
+constexpr double kNegligibleLog2 = 91.0;
+
 // The parameter-dependent constants of one problem: every PairConsts field
 // and every FinishConsts field except T and constant (which depend on the
 // event set only).  Written for host and device alike with products for the
@@ -139,10 +153,11 @@ inline void param_consts(const double* p, const ConstsSpec& s, PairConsts& c, Fi
     } else {
         c.fSh = c.fSl = c.fWh = c.fWl = 0.0f;
     }
-    const double thr = fp32 ? kSkipF32 : kSkipF64;
-    c.skipB = (s.skip && c.cB < 0.0 && c.cA <= 0.0) ? thr : -1.0;
-    c.skipS = (s.skip && c.cW < 0.0 && c.cS <= 0.0) ? thr : -1.0;
     const double kLn2 = 0.693147180559945309417232121458176568;
+    const double thr = fp32 ? kSkipF32 : kSkipF64;
+    const double thrB = s.truncate ? fmin(thr, kNegligibleLog2 * kLn2) : thr;
+    c.skipB = (s.skip && c.cB < 0.0 && c.cA <= 0.0) ? thrB : -1.0;
+    c.skipS = (s.skip && c.cW < 0.0 && c.cS <= 0.0) ? thr : -1.0;
     c.fastB = (s.fastTail && (!fp32 || (s.variant & 2)) && c.cB < 0.0 && c.cA <= 0.0)
                   ? (fp32 ? kFastTailLog2 : kFastTailLog2F64) * kLn2
                   : -1.0;

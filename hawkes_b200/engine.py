@@ -51,6 +51,7 @@ ORDERED = 1 << 13       # both orders of every background pair, either precision
 FP32_ORDERED = ORDERED  # earlier name of the same bit
 NO_INCREMENTAL = 1 << 14
 NO_FAST_TAIL = 1 << 15  # one exponential for every term, the far tail included
+NO_TAIL_TRUNCATION = 1 << 16  # skip background tile pairs only where every term underflows
 
 # Fault-injection stages (CudaHawkes.injectFault).
 FAULT_UPLOAD = 1

@@ -83,6 +83,12 @@ extern "C" {
                                                 all below 2^-12 (FP32-compensated mode) or
                                                 2^-60 (FP64 mode) of an event's own term take
                                                 those terms from ex2.approx) */
+#define HPHC_FLAG_NO_TAIL_TRUNCATION (1L << 16) /* skip background tile pairs only where
+                                                every term underflows (by default, in both
+                                                modes, tile pairs whose background terms are
+                                                all below 2^-91 of an event's own term are
+                                                skipped: together under 2^-60 of any
+                                                event's sums) */
 
 /* How the last evaluation was computed (hphc_get_last_evaluation_path). */
 #define HPHC_PATH_SWEEP 0        /* the O(N^2) pair sweep                             */
@@ -391,8 +397,10 @@ int hphc_get_last_evaluation_path(hphc_engine* engine, int* path);
 /* Kernel launches made by the most recent evaluation call (for launch
  * accounting), and how many background and self-excitation pair terms its
  * sweep evaluated.  Of the 2 N^2 possible terms the rest were skipped at tile
- * level: the non-causal half of the self-excitation sum and tile pairs whose
- * terms all underflow to exactly zero in the working precision. */
+ * level: the non-causal half of the self-excitation sum, tile pairs whose
+ * terms all underflow to exactly zero in the working precision, and (tail
+ * truncation) background tile pairs whose terms are all below 2^-91 of an
+ * event's own term. */
 int hphc_get_last_launch_stats(hphc_engine* engine, int* kernelLaunches,
                                double* backgroundTerms, double* selfExciteTerms);
 

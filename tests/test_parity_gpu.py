@@ -154,7 +154,8 @@ def test_underflow_skip_is_bit_exact(flags):
     # must give identical bits.
     loc, t = workloads.uniform(20000, seed=7)
     p = workloads.BASE_PARAMS
-    with engine(loc, t, p, flags) as a, engine(loc, t, p, flags | hb.NO_UNDERFLOW_SKIP) as b:
+    with engine(loc, t, p, flags | hb.NO_TAIL_TRUNCATION) as a, \
+            engine(loc, t, p, flags | hb.NO_UNDERFLOW_SKIP) as b:
         a.setSweepShape(2, 16)  # same summation order in both
         b.setSweepShape(2, 16)
         la, ga = a.getLogLikelihoodAndGradient()
@@ -166,6 +167,31 @@ def test_underflow_skip_is_bit_exact(flags):
     assert la == lb and np.array_equal(ga, gb) and np.array_equal(pa, pb)
     assert nba + nsa < nbb + nsb  # the skip did remove work
     assert nbb == 20000.0 ** 2  # without it every background term is evaluated
+
+
+@pytest.mark.parametrize("flags", MODES, ids=IDS)
+def test_tail_truncation_is_below_fp64_rounding(flags):
+    # Background tile pairs whose terms are all below 2^-91 of an event's own
+    # term are skipped by default: each event's sums move by under 2^-60.
+    loc, t = workloads.uniform(20000, seed=7)
+    p = workloads.BASE_PARAMS
+    with engine(loc, t, p, flags) as a, engine(loc, t, p, flags | hb.NO_TAIL_TRUNCATION) as b:
+        a.setSweepShape(2, 16)
+        b.setSweepShape(2, 16)
+        la, ga = a.getLogLikelihoodAndGradient()
+        lb, gb = b.getLogLikelihoodAndGradient()
+        _, nba, nsa = a.lastLaunchStats()
+        _, nbb, nsb = b.lastLaunchStats()
+        pa, pb = a.getProbsSelfExcite(), b.getProbsSelfExcite()
+    assert abs(la - lb) <= 1e-14 * abs(lb)
+    assert np.all(np.abs(ga - gb) <= 1e-12 * np.max(np.abs(gb)))
+    assert np.all(np.abs(pa - pb) <= 1e-15)
+    assert nsa == nsb  # the self-excitation sums keep the underflow skip only
+    # times span 8760 h and b = 1/336 per hour: pairs more than 11.2 / b =
+    # 3774 h apart are cut (FP32 underflow alone cuts at 13.3 / b, FP64 never)
+    gap = np.abs(t[:, None] - t[None, ::50])
+    assert nba < np.mean(gap < 3774 * 1.1) * 20000.0 ** 2
+    assert nba < nbb
 
 
 @pytest.mark.parametrize("flags", [FP64, FP32C, FP32O], ids=["fp64", "fp32c", "fp32c_ordered"])
