@@ -170,6 +170,7 @@ struct EventSet {
     bool sorted = false;
     DevBuf<double> dLoc, dTimes, dRecF64, dTileMin, dTileMax;
     DevBuf<int32_t> dRanks;
+    DevBuf<int> dTileChanges;  // FP32 mode, sorted times: ranks computed on the device
 
     cudaError_t alloc(int dim, int n, int precision) {
         D = dim;
@@ -182,7 +183,7 @@ struct EventSet {
             return e;
         if (precision == HPHC_PRECISION_FP64) {
             if ((e = dRecF64.reserve((size_t)N * 10))) return e;
-        } else if ((e = dRanks.reserve(N))) {
+        } else if ((e = dRanks.reserve(N)) || (e = dTileChanges.reserve(nTiles))) {
             return e;
         }
         std::memset(hTimes.p, 0, (size_t)N * sizeof(double));
@@ -202,6 +203,7 @@ struct EventSet {
         dTileMin.release();
         dTileMax.release();
         dRanks.release();
+        dTileChanges.release();
     }
 
     // Host-side derived data of the times: sortedness, dense ranks (equal
@@ -209,16 +211,13 @@ struct EventSet {
     // records), per-tile bounds.  Sorted times (the usual case) take one pass
     // for sortedness and ranks, and the tile bounds are each tile's first and
     // last time.
+    // Sortedness and per-tile time bounds on the host.  The dense time ranks
+    // of sorted times are computed on the device at upload; unsorted times
+    // get them here (hRanks).
     void derive_times() {
         const double* t = hTimes.p;
         bool asc = true;
-        int r = 0;
-        hRanks.p[0] = 0;
-        for (int i = 1; i < N; ++i) {
-            asc &= t[i - 1] <= t[i];
-            r += t[i] != t[i - 1];
-            hRanks.p[i] = r;
-        }
+        for (int i = 1; i < N; ++i) asc &= t[i - 1] <= t[i];
         sorted = asc;
         const int nTiles = (N + kTile - 1) / kTile;
         if (sorted) {
@@ -231,7 +230,7 @@ struct EventSet {
         std::vector<int> idx(N);
         std::iota(idx.begin(), idx.end(), 0);
         std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return t[x] < t[y]; });
-        r = 0;
+        int r = 0;
         for (int k = 0; k < N; ++k) {
             if (k > 0 && t[idx[k]] != t[idx[k - 1]]) ++r;
             hRanks.p[idx[k]] = r;
@@ -259,11 +258,16 @@ struct EventSet {
         if (precision == HPHC_PRECISION_FP64) {
             e = launch_pack_f64(D, N, dLoc.p, dTimes.p, dRecF64.p, dTileMin.p, dTileMax.p, s);
             *launches += 2;
+        } else if (sorted) {
+            if ((e = launch_tile_bounds(N, dTimes.p, dTileMin.p, dTileMax.p, dTileChanges.p, s)))
+                return e;
+            e = launch_sorted_ranks(N, dTimes.p, dTileChanges.p, dRanks.p, s);
+            *launches += 3;
         } else {
             if ((e = cudaMemcpyAsync(dRanks.p, hRanks.p, (size_t)N * sizeof(int32_t),
                                      cudaMemcpyHostToDevice, s)))
                 return e;
-            e = launch_tile_bounds(N, dTimes.p, dTileMin.p, dTileMax.p, s);
+            e = launch_tile_bounds(N, dTimes.p, dTileMin.p, dTileMax.p, nullptr, s);
             *launches += 1;
         }
         return e;

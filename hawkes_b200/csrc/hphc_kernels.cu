@@ -80,14 +80,26 @@ __global__ void pack_f32_jobs_kernel(const PackJob* __restrict__ jobs) {
     for (int k = 2 * D + 3; k < S; ++k) r[k] = 0.0f;
 }
 
-// One CTA of kTile threads per tile: min and max of t over the tile.
+// 1 where event j's time differs from event j-1's (j > 0): for sorted times
+// the dense rank of t_j is the number of such events in 1..j.
+__device__ __forceinline__ int time_changes(int N, const double* __restrict__ times, int j) {
+    return (j > 0 && j < N && times[j] != times[j - 1]) ? 1 : 0;
+}
+
+// One CTA of kTile threads per tile: min and max of t over the tile, and
+// (tileChanges non-null) the tile's count of time changes.
 __global__ void __launch_bounds__(kTile)
 tile_bounds_kernel(int N, const double* __restrict__ times, double* __restrict__ tileMin,
-                   double* __restrict__ tileMax) {
+                   double* __restrict__ tileMax, int* __restrict__ tileChanges) {
     __shared__ double sMin[kTile / 32], sMax[kTile / 32];
+    __shared__ int sChanges[kTile / 32];
     const int j = blockIdx.x * kTile + threadIdx.x;
     double lo = INFINITY, hi = -INFINITY;
     if (j < N) lo = hi = times[j];
+    if (tileChanges) {
+        const int c = __reduce_add_sync(0xffffffffu, time_changes(N, times, j));
+        if ((threadIdx.x & 31) == 0) sChanges[threadIdx.x >> 5] = c;
+    }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         lo = fmin(lo, __shfl_down_sync(0xffffffffu, lo, o));
@@ -106,7 +118,70 @@ tile_bounds_kernel(int N, const double* __restrict__ times, double* __restrict__
         }
         tileMin[blockIdx.x] = lo;
         tileMax[blockIdx.x] = hi;
+        if (tileChanges) {
+            int c = 0;
+            for (int k = 0; k < kTile / 32; ++k) c += sChanges[k];
+            tileChanges[blockIdx.x] = c;
+        }
     }
+}
+
+// One CTA of 1024 threads: v[0..n) replaced by its exclusive prefix sums
+// (the first time change of each tile), in chunks of 1024 with a carry.
+__global__ void __launch_bounds__(1024) exclusive_scan_kernel(int n, int* __restrict__ v) {
+    __shared__ int sWarp[32];
+    __shared__ int sTotal;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int carry = 0;
+    for (int base = 0; base < n; base += 1024) {
+        const int i = base + threadIdx.x;
+        const int x = i < n ? v[i] : 0;
+        int s = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += y;
+        }
+        if (lane == 31) sWarp[w] = s;
+        __syncthreads();
+        if (w == 0) {
+            const int ws = sWarp[lane];
+            int t = ws;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, t, o);
+                if (lane >= o) t += y;
+            }
+            sWarp[lane] = t - ws;  // this warp's offset within the chunk
+            if (lane == 31) sTotal = t;
+        }
+        __syncthreads();
+        if (i < n) v[i] = carry + sWarp[w] + s - x;
+        carry += sTotal;
+        __syncthreads();  // sWarp and sTotal are rewritten by the next chunk
+    }
+}
+
+// One CTA of kTile threads per tile: rank[j] = tileOffset[tile] (the time
+// changes before the tile) + the changes at the tile's events up to j (an
+// inclusive scan within the tile).
+__global__ void __launch_bounds__(kTile)
+sorted_ranks_kernel(int N, const double* __restrict__ times, const int* __restrict__ tileOffset,
+                    int32_t* __restrict__ ranks) {
+    __shared__ int sWarp[kTile / 32];
+    const int j = blockIdx.x * kTile + threadIdx.x;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int s = time_changes(N, times, j);
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, s, o);
+        if (lane >= o) s += y;
+    }
+    if (lane == 31) sWarp[w] = s;
+    __syncthreads();
+    int before = 0;
+    for (int k = 0; k < w; ++k) before += sWarp[k];
+    if (j < N) ranks[j] = tileOffset[blockIdx.x] + before + s;
 }
 
 // ------------------------------------------------------ tile-pair decision --
@@ -1273,13 +1348,23 @@ cudaError_t launch_pack_f64(int D, int N, const double* loc, const double* times
 #undef X
         default: return cudaErrorInvalidValue;
     }
-    tile_bounds_kernel<<<(N + kTile - 1) / kTile, kTile, 0, s>>>(N, times, tileMin, tileMax);
+    tile_bounds_kernel<<<(N + kTile - 1) / kTile, kTile, 0, s>>>(N, times, tileMin, tileMax,
+                                                                  nullptr);
     return cudaGetLastError();
 }
 
 cudaError_t launch_tile_bounds(int N, const double* times, double* tileMin, double* tileMax,
-                               cudaStream_t s) {
-    tile_bounds_kernel<<<(N + kTile - 1) / kTile, kTile, 0, s>>>(N, times, tileMin, tileMax);
+                               int* tileChanges, cudaStream_t s) {
+    tile_bounds_kernel<<<(N + kTile - 1) / kTile, kTile, 0, s>>>(N, times, tileMin, tileMax,
+                                                                  tileChanges);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sorted_ranks(int N, const double* times, int* tileChanges, int32_t* ranks,
+                                cudaStream_t s) {
+    const int nTiles = (N + kTile - 1) / kTile;
+    exclusive_scan_kernel<<<1, 1024, 0, s>>>(nTiles, tileChanges);
+    sorted_ranks_kernel<<<nTiles, kTile, 0, s>>>(N, times, tileChanges, ranks);
     return cudaGetLastError();
 }
 

@@ -205,8 +205,15 @@ struct SweepGeometry {
 // compute per-tile time bounds.  ranks may be null for the FP64 layout.
 cudaError_t launch_pack_f64(int D, int N, const double* loc, const double* times, double* rec,
                             double* tileMin, double* tileMax, cudaStream_t s);
+// Per-tile time bounds; tileChanges (nullable) receives each tile's count of
+// events whose time differs from the previous event's.
 cudaError_t launch_tile_bounds(int N, const double* times, double* tileMin, double* tileMax,
-                               cudaStream_t s);
+                               int* tileChanges, cudaStream_t s);
+// Dense time ranks of SORTED times from the tile counts of launch_tile_bounds
+// (which it overwrites with their exclusive prefix sums): rank[j] = number of
+// k in 1..j with t_k != t_{k-1}.  Two launches.
+cudaError_t launch_sorted_ranks(int N, const double* times, int* tileChanges, int32_t* ranks,
+                                cudaStream_t s);
 
 // Pair sweep: fills partials[chunk][6][Npad] with unit pair sums.  R is the
 // number of target events per thread (strip = kSweepThreads * R events).

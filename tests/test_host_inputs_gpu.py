@@ -47,3 +47,32 @@ def test_rejected_large_input_changes_nothing():
         assert ei.value.status == 4 and str(2 * (n - 7) + 1) in str(ei.value)
         assert e.getSumOfLikContribs() == ll0
         assert e.lastEvaluationPath == hb.PATH_KEPT_SUMS
+
+
+def test_ranks_follow_sorted_and_unsorted_times():
+    # Sorted times get their dense ranks on the device, unsorted ones from the
+    # host: switching between the two on one engine must match fresh engines.
+    n = 20000
+    loc, t = workloads.uniform(n, seed=42)
+    tied = np.floor(t / 3.0) * 3.0
+    rng = np.random.default_rng(43)
+    perm = rng.permutation(n - 1)  # the last event keeps the latest time (T)
+    shuffled_t = np.concatenate([tied[:-1][perm], tied[-1:]])
+    shuffled_loc = np.concatenate([loc[:-1][perm], loc[-1:]])
+    p = np.asarray(workloads.BASE_PARAMS)
+    cases = [(tied, loc), (shuffled_t, shuffled_loc), (t, loc), (tied, loc)]
+
+    def run(e, tt, ll):
+        e.setTimesData(tt)
+        e.updateLocations(-1, ll)
+        e.setParameters(p)
+        return e.getLogLikelihoodAndGradient()
+
+    with hb.CudaHawkes(2, n, hb.CUDA | hb.COMPENSATED, 0) as e:
+        got = [run(e, tt, ll) for tt, ll in cases]
+    for (tt, ll), (lg, gg) in zip(cases, got):
+        with hb.CudaHawkes(2, n, hb.CUDA | hb.COMPENSATED, 0) as f:
+            lf, gf = run(f, tt, ll)
+        assert lg == lf and np.array_equal(gg, gf)
+    # the permuted events are the same set: equal up to summation order
+    assert abs(got[1][0] - got[0][0]) <= 5e-9 * abs(got[0][0])

