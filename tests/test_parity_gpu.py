@@ -302,3 +302,22 @@ def test_r_time_test():
         hb.timeTest(locationCount=100, r=True)
     with pytest.raises(hb.HawkesError):
         hb.timeTest(locationCount=100, gpu=0)
+
+
+@pytest.mark.parametrize("flags", [FP64, FP32C], ids=["fp64", "fp32c"])
+def test_tail_truncation_at_random_parameters(flags):
+    # Parameters spread log-normally (sd 1) around the base, so the time
+    # kernel ranges from wide (little cut) to sharp (most tile pairs cut).
+    loc, t = workloads.uniform(6000, seed=11)
+    rng = np.random.default_rng(12)
+    for k in range(6):
+        p = workloads.BASE_PARAMS * np.exp(rng.normal(0.0, 1.0, 6))
+        with engine(loc, t, p, flags) as a, engine(loc, t, p, flags | hb.NO_TAIL_TRUNCATION) as b:
+            a.setSweepShape(2, 16)
+            b.setSweepShape(2, 16)
+            la, ga = a.getLogLikelihoodAndGradient()
+            lb, gb = b.getLogLikelihoodAndGradient()
+            pa, pb = a.getProbsSelfExcite(), b.getProbsSelfExcite()
+        assert abs(la - lb) <= 1e-14 * abs(lb), k
+        assert np.all(np.abs(ga - gb) <= 1e-12 * np.max(np.abs(gb))), k
+        assert np.all(np.abs(pa - pb) <= 1e-15), k
