@@ -30,10 +30,12 @@ _ref = None
 
 
 def build(reference_src: str | None = None) -> None:
-    """Build liboracle.so, and the reference artefacts when the sources exist."""
+    """Build liboracle.so, and the reference artefacts when the reference's
+    src/ directory is given (argument, else the HAWKES_REF_SRC environment
+    variable) and exists."""
     subprocess.run(["make", "-C", HERE, "oracle"], check=True, stdout=subprocess.DEVNULL)
-    src = reference_src or "/root/reference/src"
-    if os.path.isdir(src):
+    src = reference_src or os.environ.get("HAWKES_REF_SRC", "")
+    if src and os.path.isdir(src):
         subprocess.run(["make", "-C", HERE, "ref", f"REF_SRC={src}"], check=True,
                        stdout=subprocess.DEVNULL)
 
