@@ -55,19 +55,17 @@ N_EVENTS = 100000
 SEED = 5
 L2_FLUSH_BYTES = 256 << 20
 
-# Algorithmic work of the brute-force pair sum (FMA = 1 instruction): every
-# ordered pair (i, j) has a background term, 11 FP32 instructions (dx, dy, dt;
-# d^2; exponent; three weighted sums) + 1 ex2; the causal half has a
-# self-excitation term, 5 FP32 (exponent; three weighted sums) + 1 ex2.  Per
-# pair-eval: 11 + 5/2 = 13.5 FP32 instructions and 1.5 ex2.  The roofline
-# counts this per-pair figure times the N^2 pair-evals one sweep launch
-# stands for, so it credits the tile-level skips (non-causal half, exact
-# underflow, one exponential for both orders of a background pair) as work
-# done; "evaluated" below counts only the terms the launch computed.
+# Algorithmic work (FMA = 1 instruction).  The roofline counts the terms a
+# sweep launch evaluated: a background exponential costs 11 FP32 instructions
+# (dx, dy, dt; d^2; exponent; three weighted sums) + 1 ex2, and 3 more (the
+# other event's three weighted sums) when one evaluation serves both events
+# of a pair; a self-excitation term costs 5 (exponent; three weighted sums) +
+# 1 ex2.  The brute-force sum over every ordered pair would cost 11 + 5/2 =
+# 13.5 FP32 instructions and 1.5 ex2 per pair-eval; the sweep skips the
+# non-causal half, exact underflows, the truncated background tail and one
+# order of each background pair, so that count ("effective") is a rate
+# equivalent and can exceed the pipe's peak.
 FP32_PER_PAIR_EVAL, EX2_PER_PAIR_EVAL = 13.5, 1.5
-# Per evaluated term: background exponential 11, plus 3 (the column's three
-# weighted sums) when one evaluation serves both events of a pair;
-# self-excitation term 5.
 FP32_PER_B, FP32_PER_COL, FP32_PER_S = 11.0, 3.0, 5.0
 FP32_LANES_PER_SM = 128
 MUFU_LANES_PER_SM = 16
@@ -151,37 +149,58 @@ class ClockSampler:
 
 # ------------------------------------------------------------ reference arm --
 
+def load_workloads():
+    """hawkes_b200/workloads.py loaded by path, without importing the
+    hawkes_b200 package (whose __init__ loads the CUDA library): the CPU arms
+    map only the reference engine."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "_hawkes_workloads", os.path.join(ROOT, "hawkes_b200", "workloads.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def headline_config(world, n=N_EVENTS):
+    """The config object both arms print: the same events, sizes and
+    parameters."""
+    return {"workload": f"uniform N={n} D=2, 20x20 km, [0,8760) h sorted, seed {SEED}, "
+                        "base params (sigma=1, tauX=1/1.6, tauT=1/336, omega=1, theta=1, mu0=1)",
+            "N": n, "D": 2,
+            "l2": "GPU arm: flushed before every timed step (256 MiB device write, outside the "
+                  "timing); CPU arm: host memory",
+            "parallelism": f"replicas x{world}"}
+
+
 def reference_arm(args):
+    """The reference's own CPU engine (NewHawkes, double, its TBB path over
+    all host cores; src/NewHawkes.hpp:812-848) on the headline events: every
+    timed step is one full N = 100,000 evaluation.  Warm-up steps evaluate
+    the first 20,000 events (they only warm the thread pool and caches)."""
     rank = env_int("RANK", 0)
     if rank != 0:
         return 0
     import oracle
-    from hawkes_b200 import workloads
 
+    wl = load_workloads()
     cores = os.cpu_count() or 1
     if not oracle.ref_available():
         print(json.dumps({"impl": "reference",
                           "unavailable": "reference CPU engine (oracle/_ref) not built"}))
         return 0
-    # Calibrate the sample size so the whole run (warm-up + steps) takes about
-    # two minutes on this host, and no step more than ~6 s.
-    step_s = min(6.0, 120.0 / max(1, args.steps + args.warmup))
-    loc, t = workloads.uniform(4000, seed=SEED)
-    eng = oracle.RefEngine(2, 4000, threads=cores)
-    eng.set_data(loc, t)
-    eng.set_parameters(workloads.BASE_PARAMS)
-    t0 = time.perf_counter()
-    eng.loglik()
-    rate = 4000.0 ** 2 / (time.perf_counter() - t0)
-    eng.close()
-    n = int(min(N_EVENTS, max(2000, math.sqrt(step_s * rate)) // 1000 * 1000))
-    loc, t = workloads.uniform(n, seed=SEED)
+    n = args.n
+    loc, t = wl.uniform(n, seed=SEED)
+    nw = min(n, 20000)
+    warm = oracle.RefEngine(2, nw, threads=cores)
+    warm.set_data(loc[:nw], t[:nw])
+    warm.set_parameters(wl.BASE_PARAMS)
+    for _ in range(args.warmup):
+        warm.loglik()
+    warm.close()
     eng = oracle.RefEngine(2, n, threads=cores)
     variant = eng.variant.splitlines()[0]
     eng.set_data(loc, t)
-    eng.set_parameters(workloads.BASE_PARAMS)
-    for _ in range(args.warmup):
-        eng.loglik()
+    eng.set_parameters(wl.BASE_PARAMS)
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
@@ -189,16 +208,15 @@ def reference_arm(args):
         times.append(time.perf_counter() - t0)
     eng.close()
     ms = 1e3 * statistics.mean(times)
-    value = n * n / (ms / 1e3)
-    sample = (f"N={n} events of the same generator (uniform 20x20 km, [0,8760) h, seed {SEED}); "
+    value = float(n) * n / (ms / 1e3)
+    sample = (f"{args.steps} full evaluations at N={n} (the headline events, seed {SEED}); "
               f"log-likelihood only (the reference has no gradient); {variant}, {cores} threads")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic",
-        "config": {"workload": f"uniform N={n} D=2 (bounded sample of N={N_EVENTS}), base params,"
-                               " loglik", "N": n, "D": 2},
+        "data": "synthetic", "computes": "log-likelihood (the reference has no gradient)",
+        "config": headline_config(args.gpus, n),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -206,40 +224,34 @@ def reference_arm(args):
     return 0
 
 
-def cpu_baseline(budget_s=15.0):
-    """The reference CPU engine (or the oracle port when it is not built) on
-    a bounded sample, all host cores."""
+def cpu_baseline(n=N_EVENTS):
+    """The reference CPU engine (or the oracle port when it is not built):
+    one full evaluation of the headline events on all host cores."""
     import oracle
-    from hawkes_b200 import workloads
 
+    wl = load_workloads()
     cores = os.cpu_count() or 1
     kind = "reference" if oracle.ref_available() else "port"
-    loc, t = workloads.uniform(4000, seed=SEED)
+    loc, t = wl.uniform(n, seed=SEED)
     if kind == "reference":
-        def evaluate(loc, t):
-            e = oracle.RefEngine(2, len(t), threads=cores)
-            e.set_data(loc, t)
-            e.set_parameters(workloads.BASE_PARAMS)
-            t0 = time.perf_counter()
-            e.loglik()
-            dt = time.perf_counter() - t0
-            v = e.variant.splitlines()[0]
-            e.close()
-            return dt, v
+        e = oracle.RefEngine(2, n, threads=cores)
+        e.set_data(loc, t)
+        e.set_parameters(wl.BASE_PARAMS)
+        t0 = time.perf_counter()
+        e.loglik()
+        dt = time.perf_counter() - t0
+        variant = e.variant.splitlines()[0]
+        e.close()
+        what = "log-likelihood only (the reference has no gradient)"
     else:
-        def evaluate(loc, t):
-            t0 = time.perf_counter()
-            oracle.oracle_eval(loc, t, workloads.BASE_PARAMS, threads=cores)
-            return time.perf_counter() - t0, "oracle port (C, FP64, long double sums)"
-    dt, _ = evaluate(loc, t)
-    rate = 4000.0 ** 2 / dt
-    n = int(min(N_EVENTS, max(4000, math.sqrt(budget_s * rate)) // 1000 * 1000))
-    loc, t = workloads.uniform(n, seed=SEED)
-    dt, variant = evaluate(loc, t)
-    what = "log-likelihood only (the reference has no gradient)" if kind == "reference" else \
-        "log-likelihood + gradient"
-    return {"value": n * n / dt, "unit": UNIT, "cores": cores, "kind": kind,
-            "sample": f"one evaluation at N={n} (same generator, seed {SEED}), {what}; {variant}"}
+        t0 = time.perf_counter()
+        oracle.oracle_eval(loc, t, wl.BASE_PARAMS, threads=cores)
+        dt = time.perf_counter() - t0
+        variant = "oracle port (C, FP64, long double sums)"
+        what = "log-likelihood + gradient"
+    return {"value": float(n) * n / dt, "unit": UNIT, "cores": cores, "kind": kind,
+            "sample": f"one full evaluation at N={n} (the headline events, seed {SEED}), {what}; "
+                      f"{variant}; {dt:.1f} s"}
 
 
 # ------------------------------------------------------------------ our arm --
@@ -415,6 +427,32 @@ def make_workload(name, n):
     raise ValueError(name)
 
 
+def oracle_accuracy(res32, res64, n):
+    """Errors of both arms against the committed oracle fixture of the
+    headline events (tests/golden/headline_n100k.npz): log-likelihood
+    relative, gradient componentwise |dg_k| / |g_k| and on the per-event
+    scale sum_i |per-event contribution|."""
+    path = os.path.join(ROOT, "tests", "golden", "headline_n100k.npz")
+    if n != N_EVENTS or not os.path.exists(path):
+        return None
+    z = np.load(path)
+    ll_o, g_o, scale = float(z["oracle_loglik"]), z["oracle_grad"], z["grad_scale"]
+    out = {"reference": "oracle (C restatement, long-double sums) at N=100000; its "
+                        "log-likelihood agrees with the reference engine's to "
+                        f"{abs(ll_o - float(z['ref_loglik'])) / abs(ll_o):.1e}"
+                        if "ref_loglik" in z else "oracle (C restatement) at N=100000"}
+    for name, (ll, g) in (("fp32c", res32), ("fp64", res64)):
+        g = np.asarray(g, dtype=np.float64).reshape(-1)
+        comp = np.abs(g - g_o) / np.abs(g_o)
+        out[name] = {"loglik_rel": abs(float(ll) - ll_o) / abs(ll_o),
+                     "grad_rel_componentwise": [float(v) for v in comp],
+                     "grad_rel_per_event_scale": [float(v) for v in np.abs(g - g_o) / scale]}
+    f = out["fp32c"]
+    out["bound_1e-8_met"] = bool(f["loglik_rel"] <= 1e-8 and
+                                 max(f["grad_rel_componentwise"]) <= 1e-8)
+    return out
+
+
 def ours_arm(args):
     import torch
 
@@ -485,10 +523,12 @@ def ours_arm(args):
     peak_inst = sm_count * FP32_LANES_PER_SM * max_mhz * 1e6 / 1e12
     peak_ex2 = sm_count * MUFU_LANES_PER_SM * max_mhz * 1e6 / 1e12
     sweep_mean = statistics.mean(sweep32)
-    achieved = FP32_PER_PAIR_EVAL * pairs / (sweep_mean / 1e3) / 1e12
-    achieved_ex2 = EX2_PER_PAIR_EVAL * pairs / (sweep_mean / 1e3) / 1e12
+    # the roofline counts the terms the launch evaluated; "effective" counts
+    # the brute-force work (every ordered pair) the launch stands for
     inst = FP32_PER_B * nev + FP32_PER_COL * (nb - nev) + FP32_PER_S * ns
-    achieved_eval = inst / (sweep_mean / 1e3) / 1e12
+    achieved = inst / (sweep_mean / 1e3) / 1e12
+    achieved_ex2 = (nev + ns) / (sweep_mean / 1e3) / 1e12
+    effective = FP32_PER_PAIR_EVAL * pairs / (sweep_mean / 1e3) / 1e12
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "sweep_traffic.json")
     if os.path.exists(tpath):
@@ -507,47 +547,55 @@ def ours_arm(args):
               (f"<D=2, R={shape32[0]}>, {shape32[1]} items/SM" if shape32 else ""))
     metric = METRIC if args.workload == "headline" else \
         f"pair-evals/s loglik+grad, {args.workload}: FP32-comp vs FP64 plain"
+    config = headline_config(world, args.n) if args.workload == "headline" \
+        else dict({"workload": w["desc"],
+                   "l2": "flushed before every timed step (256 MiB write, outside the timing)",
+                   "parallelism": f"replicas x{world}"}, **w["config"])
     out = {
         "metric": metric, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step32, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 pair terms (compensated), f64 reductions", "data": "synthetic",
-        "config": dict({"workload": w["desc"], "precision": "fp32-compensated",
-                        "l2": "flushed before every timed step (256 MiB write, outside the "
-                              "timing)",
-                        "parallelism": f"replicas x{world}"}, **w["config"]),
+        "computes": "log-likelihood + 6-parameter gradient",
+        "config": config,
         "fp64_plain": {"value": value64, "ms_per_step": ms_step64,
                        "sweep_ms": statistics.mean(sweep64), "steps": steps64,
                        "terms": {"background": nb64, "self_excitation": ns64}},
         "speedup_fp32c_vs_fp64": value / value64,
         "accuracy": acc,
+        "accuracy_vs_oracle": (oracle_accuracy((res32[0], res32[1]), (res64[0], res64[1]), args.n)
+                               if w["kind"] == "single" and args.workload == "headline" else None),
         "terms": {"background": nb, "self_excitation": ns, "possible": 2 * pairs,
                   "background_exponentials": nev,
                   "note": "pair terms the sweep accounted for; the rest are the non-causal half "
                           "of the self-excitation sum, self-excitation tile pairs whose terms "
                           "are all exactly zero in FP32, and background tile pairs whose terms "
-                          "are all below 2^-91 of an event's own term (tail truncation: under "
-                          "2^-60 of any event's sums).  A background pair with the other event "
-                          "in an earlier "
-                          "tile is evaluated once (one exponential) for both events"},
+                          "are all below 2^-60 of an event's own term (tail truncation of the "
+                          "FP32 modes: under 2^-33 of any event's sums).  A background pair with the other event "
+                          "in an earlier tile is evaluated once (one exponential) for both "
+                          "events"},
         "roofline": {"bound": "fp32", "kernel": kernel,
                      "achieved": achieved, "peak": peak_inst, "unit": "Tinst/s",
                      "frac": achieved / peak_inst, "traffic": traffic,
-                     "count": f"{FP32_PER_PAIR_EVAL} FP32 instructions (FMA = 1) per pair-eval "
-                              "(11 background on every ordered pair + 5 self-excitation on the "
-                              f"causal half) x {pairs:.4g} pair-evals per sweep launch, over the "
-                              "mean CUDA-event duration of the sweep kernel",
+                     "count": "FP32 instructions (FMA = 1) of the terms this launch evaluated: "
+                              f"{FP32_PER_B:g} per background exponential, {FP32_PER_COL:g} per "
+                              "background pair also added to the earlier event's sums, "
+                              f"{FP32_PER_S:g} per self-excitation term; over the mean "
+                              "CUDA-event duration of the sweep kernel",
+                     "instructions_per_launch": inst,
                      "peak_source": f"{sm_count} SMs x 128 FP32 lanes x {max_mhz:.0f} MHz "
                                     f"(sm_max_mhz, {peak_src})",
                      "ex2": {"achieved": achieved_ex2, "peak": peak_ex2, "unit": "Tex2/s",
                              "frac": achieved_ex2 / peak_ex2,
-                             "count": f"{EX2_PER_PAIR_EVAL} ex2 per pair-eval; peak {sm_count} "
-                                      f"SMs x 16 MUFU lanes x {max_mhz:.0f} MHz"},
-                     "evaluated": {"achieved": achieved_eval, "frac": achieved_eval / peak_inst,
-                                   "count": "only the terms this launch computed: 11 per "
-                                            "background exponential + 3 per pair also added to "
-                                            "the earlier event's sums + 5 per self-excitation "
-                                            "term"},
+                             "count": "one MUFU ex2 per evaluated exponential; peak "
+                                      f"{sm_count} SMs x 16 MUFU lanes x {max_mhz:.0f} MHz"},
+                     "effective": {"achieved": effective, "frac_equivalent": effective / peak_inst,
+                                   "count": f"{FP32_PER_PAIR_EVAL} FP32 instructions per "
+                                            f"pair-eval x {pairs:.4g} pair-evals: the brute-force "
+                                            "work the launch stands for (it skips the non-causal "
+                                            "half, exact underflows, the truncated tail and one "
+                                            "order of each background pair), so this is a rate "
+                                            "equivalent, not pipe utilisation"},
                      "sweep_ms": sweep_mean},
         "e2e": {"value": whole_job_rate(world, pairs, 1e3 * e2e_s), "unit": UNIT,
                 "h2d_bytes_per_step": w["h2d"], "d2h_bytes_per_step": w["d2h"]},
@@ -593,7 +641,8 @@ def shard_arm(args):
         sh.getLogLikelihoodAndGradient()
     # launches of one step: the share's sweep, the rank-ordered sum, the finish
     sh.sweep()
-    n_sweep = eng.lastLaunchStats()[0]
+    n_sweep, nb_share, ns_share = eng.lastLaunchStats()
+    nev_share = eng.lastLaunchEvals()
     res = eng.getLogLikelihoodAndGradient()
     launches = n_sweep + 1 + eng.lastLaunchStats()[0]
     step_ms, sweep_ms = [], []
@@ -638,7 +687,8 @@ def shard_arm(args):
     sm_count = torch.cuda.get_device_properties(local).multi_processor_count
     max_mhz = float(peaks.get("sm_max_mhz", 1965.0))
     peak_inst = sm_count * FP32_LANES_PER_SM * max_mhz * 1e6 / 1e12
-    achieved = FP32_PER_PAIR_EVAL * pairs / world / (sweep_max / 1e3) / 1e12
+    inst = FP32_PER_B * nev_share + FP32_PER_COL * (nb_share - nev_share) + FP32_PER_S * ns_share
+    achieved = inst / (sweep_max / 1e3) / 1e12
     out = {
         "metric": METRIC, "value": pairs / (ms / 1e3), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
@@ -656,9 +706,11 @@ def shard_arm(args):
         "roofline": {"bound": "fp32", "kernel": "sweep_f32c_list_kernel (one rank's share)",
                      "achieved": achieved, "peak": peak_inst, "unit": "Tinst/s",
                      "frac": achieved / peak_inst, "traffic": None,
-                     "count": f"{FP32_PER_PAIR_EVAL} FP32 instructions per pair-eval x "
-                              f"{pairs:.4g} / {world} pair-evals per rank, over the slowest "
-                              "rank's mean sweep duration",
+                     "count": "FP32 instructions of the terms rank 0's share evaluated "
+                              f"({FP32_PER_B:g} per background exponential, {FP32_PER_COL:g} per "
+                              f"pair also added to the earlier event, {FP32_PER_S:g} per "
+                              "self-excitation term), over the slowest rank's mean sweep "
+                              "duration",
                      "peak_source": f"{sm_count} SMs x 128 FP32 lanes x {max_mhz:.0f} MHz "
                                     f"(sm_max_mhz, {peak_src})",
                      "sweep_ms": sweep_max},

@@ -9,7 +9,7 @@ from .engine import (  # noqa: F401
     NO_UNDERFLOW_SKIP,
     OPENCL, PARAMETER_NAMES, PATH_INCREMENTAL, PATH_KEPT_SUMS, PATH_SELF_EXCITATION,
     PATH_SWEEP,
-    PRECISION_FP32_COMP, PRECISION_FP64, SSE, TBB, CudaHawkes, Engine, HawkesError, Multiset,
+    PRECISION_FP32, PRECISION_FP32_COMP, PRECISION_FP64, SSE, TBB, CudaHawkes, Engine, HawkesError, Multiset,
     createEngine, engineInitial, factory, getGradient, getLogLikelihood, getProbsSelfExcite,
     setParameters, setTimesData, timeTest, updateLocations)
 from .sampler import Potential, Sampler, log_prior, sampler  # noqa: F401

@@ -52,6 +52,9 @@ SIGNATURES = {
     "hphc_set_unit_sums": (ctypes.c_int, [_handle, ctypes.c_void_p, ctypes.c_int,
                                           ctypes.c_size_t]),
     "hphc_inject_fault": (ctypes.c_int, [_handle, ctypes.c_int, ctypes.c_int]),
+    "hphc_eval_exponentials": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_float),
+                                              ctypes.c_size_t, ctypes.POINTER(ctypes.c_float),
+                                              ctypes.POINTER(ctypes.c_float)]),
     "hphc_set_kernel_timing": (ctypes.c_int, [_handle, ctypes.c_int]),
     "hphc_set_sweep_shape": (ctypes.c_int, [_handle, ctypes.c_int, ctypes.c_int]),
     "hphc_get_sweep_shape": (ctypes.c_int, [_handle, _c_int_p, _c_int_p]),

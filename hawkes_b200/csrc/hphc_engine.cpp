@@ -98,11 +98,15 @@ struct HostBuf {
         p = nullptr;
         n = 0;
     }
+    void swap(HostBuf& o) {
+        std::swap(p, o.p);
+        std::swap(n, o.n);
+    }
 };
 
 // Mean relative error of ex2.approx.ftz.f32 (the instruction rounds low on
 // average), measured once per device over 2^20 arguments spread over [-16, 0)
-// and cached.  The hardware-exponential mode divides it out of its sums.
+// and cached.  FP32 modes divide it out of the terms that come from it.
 constexpr int kMaxDevices = 64;
 constexpr int kEx2Samples = 1 << 20;
 std::mutex gEx2Mutex;
@@ -143,16 +147,22 @@ struct Mode {
     bool underflowSkip = true;
     bool symmetric = true;  // each background pair evaluated once for both events
     bool fastTail = true;   // far-tail background tile pairs on the hardware exponential
-    bool truncateTail = true;  // background tile pairs below 2^-91 of B_ii skipped
+    bool truncateTail = true;  // background tile pairs below 2^-91 (FP32: 2^-60) of B_ii skipped
 };
 
 Mode mode_from_flags(long fl) {
     Mode m;
-    m.precision = (fl & (HPHC_FLAG_FLOAT | HPHC_FLAG_COMPENSATED)) ? HPHC_PRECISION_FP32_COMP
-                                                                   : HPHC_PRECISION_FP64;
+    // COMPENSATED (with or without FLOAT): FP32 pair terms with compensated
+    // sums and FP64 reductions; FLOAT alone: FP32 throughout, the reference's
+    // single precision (src/factory.cpp:34, :45).
+    m.precision = (fl & HPHC_FLAG_COMPENSATED) ? HPHC_PRECISION_FP32_COMP
+                  : (fl & HPHC_FLAG_FLOAT)     ? HPHC_PRECISION_FP32
+                                               : HPHC_PRECISION_FP64;
     m.underflowSkip = !(fl & HPHC_FLAG_NO_UNDERFLOW_SKIP);
-    m.variant = ((fl & HPHC_FLAG_FP32_SPACE_HILO) ? 1 : 0) |
-                ((fl & HPHC_FLAG_FP32_FAST_EXP) ? 0 : 2);
+    m.variant = m.precision == HPHC_PRECISION_FP32
+                    ? 8  // plain: hardware exponential, hi parts, plain sums
+                    : ((fl & HPHC_FLAG_FP32_SPACE_HILO) ? 1 : 0) |
+                          ((fl & HPHC_FLAG_FP32_FAST_EXP) ? 0 : 2);
     m.symmetric = !(fl & HPHC_FLAG_ORDERED);
     m.fastTail = !(fl & HPHC_FLAG_NO_FAST_TAIL);
     m.truncateTail = !(fl & HPHC_FLAG_NO_TAIL_TRUNCATION);
@@ -168,13 +178,16 @@ struct EventSet {
     HostBuf<int32_t> hRanks;
     std::vector<double> hTileMin, hTileMax;
     bool sorted = false;
+    bool floatTimes = false;  // plain FP32 mode: causality from the times rounded to FP32
     DevBuf<double> dLoc, dTimes, dRecF64, dTileMin, dTileMax;
     DevBuf<int32_t> dRanks;
     DevBuf<int> dTileChanges;  // FP32 mode, sorted times: ranks computed on the device
+    DevBuf<int32_t> dOrder2, dOrder4;  // FP32 mode: spatial row order of R = 2 and 4 strips
 
     cudaError_t alloc(int dim, int n, int precision) {
         D = dim;
         N = n;
+        floatTimes = precision == HPHC_PRECISION_FP32;
         const int nTiles = (N + kTile - 1) / kTile;
         cudaError_t e;
         if ((e = hTimes.reserve(N)) || (e = hRanks.reserve(N)) ||
@@ -183,7 +196,8 @@ struct EventSet {
             return e;
         if (precision == HPHC_PRECISION_FP64) {
             if ((e = dRecF64.reserve((size_t)N * 10))) return e;
-        } else if ((e = dRanks.reserve(N)) || (e = dTileChanges.reserve(nTiles))) {
+        } else if ((e = dRanks.reserve(N)) || (e = dTileChanges.reserve(nTiles)) ||
+                   (e = dOrder2.reserve(N)) || (e = dOrder4.reserve(N))) {
             return e;
         }
         std::memset(hTimes.p, 0, (size_t)N * sizeof(double));
@@ -204,6 +218,8 @@ struct EventSet {
         dTileMax.release();
         dRanks.release();
         dTileChanges.release();
+        dOrder2.release();
+        dOrder4.release();
     }
 
     // Host-side derived data of the times: sortedness, dense ranks (equal
@@ -214,10 +230,11 @@ struct EventSet {
     // Sortedness and per-tile time bounds on the host.  The dense time ranks
     // of sorted times are computed on the device at upload; unsorted times
     // get them here (hRanks).
-    void derive_times() {
+    void derive_times(int knownSorted = -1) {
         const double* t = hTimes.p;
-        bool asc = true;
-        for (int i = 1; i < N; ++i) asc &= t[i - 1] <= t[i];
+        bool asc = knownSorted > 0;
+        if (knownSorted < 0)
+            for (int i = 1; i < N; ++i) asc &= t[i - 1] <= t[i];
         sorted = asc;
         const int nTiles = (N + kTile - 1) / kTile;
         if (sorted) {
@@ -232,7 +249,9 @@ struct EventSet {
         std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return t[x] < t[y]; });
         int r = 0;
         for (int k = 0; k < N; ++k) {
-            if (k > 0 && t[idx[k]] != t[idx[k - 1]]) ++r;
+            const bool differs = floatTimes ? (float)t[idx[k]] != (float)t[idx[k - (k > 0)]]
+                                            : t[idx[k]] != t[idx[k - (k > 0)]];
+            if (k > 0 && differs) ++r;
             hRanks.p[idx[k]] = r;
         }
         for (int k = 0; k < nTiles; ++k) {
@@ -258,10 +277,18 @@ struct EventSet {
         if (precision == HPHC_PRECISION_FP64) {
             e = launch_pack_f64(D, N, dLoc.p, dTimes.p, dRecF64.p, dTileMin.p, dTileMax.p, s);
             *launches += 2;
-        } else if (sorted) {
-            if ((e = launch_tile_bounds(N, dTimes.p, dTileMin.p, dTileMax.p, dTileChanges.p, s)))
+            return e;
+        }
+        if ((e = launch_strip_order(D, N, 2, dLoc.p, dOrder2.p, s)) ||
+            (e = launch_strip_order(D, N, 4, dLoc.p, dOrder4.p, s)))
+            return e;
+        for (int S = 2 * kSweepThreads; S <= 4 * kSweepThreads; S *= 2)
+            *launches += (N >= S) + (N % S != 0);
+        if (sorted) {
+            if ((e = launch_tile_bounds(N, dTimes.p, dTileMin.p, dTileMax.p, dTileChanges.p, s,
+                                        floatTimes)))
                 return e;
-            e = launch_sorted_ranks(N, dTimes.p, dTileChanges.p, dRanks.p, s);
+            e = launch_sorted_ranks(N, dTimes.p, dTileChanges.p, dRanks.p, s, floatTimes);
             *launches += 3;
         } else {
             if ((e = cudaMemcpyAsync(dRanks.p, hRanks.p, (size_t)N * sizeof(int32_t),
@@ -279,6 +306,8 @@ struct EventSet {
         v.dLoc = dLoc.p;
         v.dTimes = dTimes.p;
         v.dRanks = dRanks.p;
+        v.dOrder2 = dOrder2.p;
+        v.dOrder4 = dOrder4.p;
         v.dRecF64 = dRecF64.p;
         v.dTileMin = dTileMin.p;
         v.dTileMax = dTileMax.p;
@@ -324,7 +353,11 @@ struct Runtime {
         if (!g.ok) return fmt(err, HPHC_ERR_CUDA, "cannot select device %d", device);
         cudaError_t e = cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
         if (e != cudaSuccess) return cuda_status(err, e, "create stream");
-        if (mode.precision != HPHC_PRECISION_FP64 && !(mode.variant & 2) &&
+        // FP32-compensated mode: the hardware exponential's mean relative
+        // error, divided out of every term that comes from it (all of them in
+        // the hardware-exponential variant, the far tail in the default one;
+        // the plain FP32 mode keeps it, as the reference's float engine does)
+        if (mode.precision == HPHC_PRECISION_FP32_COMP &&
             (e = ex2_bias_for_device(device, stream, &ex2Bias)) != cudaSuccess)
             return cuda_status(err, e, "exponential calibration");
         const int st = ex.init(D, mode.precision, mode.variant, mode.underflowSkip, device, stream,
@@ -365,6 +398,34 @@ bool all_finite(const double* v, size_t n, size_t* bad) {
     return true;
 }
 
+// Copies n doubles from src to dst and tests them in the same pass (one read
+// of the caller's array instead of one for the test and one for the copy):
+// false if any is not finite, with *bad the first such index (dst is then
+// partly written and must be discarded).  ASC: *ascending = src is
+// non-decreasing.
+template <bool ASC>
+bool copy_checked(const double* __restrict__ src, double* __restrict__ dst, size_t n,
+                  size_t* bad, bool* ascending) {
+    constexpr uint64_t kExp = 0x7ff0000000000000ULL;
+    uint64_t any = 0, desc = 0;
+    for (size_t i = 0; i < n; ++i) {
+        const double v = src[i];
+        uint64_t u;
+        std::memcpy(&u, &v, sizeof u);
+        any |= (uint64_t)((u & kExp) == kExp);
+        if (ASC && i > 0) desc |= (uint64_t)(src[i - 1] > v);
+        dst[i] = v;
+    }
+    if (ASC) *ascending = desc == 0;
+    if (!any) return true;
+    for (size_t i = 0; i < n; ++i)
+        if (!std::isfinite(src[i])) {
+            *bad = i;
+            return false;
+        }
+    return true;
+}
+
 }  // namespace
 
 struct hphc_engine {
@@ -379,6 +440,10 @@ struct hphc_engine {
     double sumOfLikContribs = 0.0, storedSumOfLikContribs = 0.0;
     HostBuf<double> hLoc[2];  // double-buffered location mirrors (src/NewHawkes.hpp:869-873)
     int curLoc = 0;
+    // A full new location block or time vector is copied and checked in one
+    // pass into a spare mirror, which replaces the current one only if every
+    // value is finite: a rejected input leaves the events unchanged.
+    HostBuf<double> hLocSpare, hTimesSpare;
     EventSet set;
     DevBuf<double> dProbs;
     std::vector<double> hOut;
@@ -442,7 +507,8 @@ struct hphc_engine {
         DeviceGuard g(rt.device);
         const size_t nl = (size_t)N * D;
         cudaError_t e;
-        if ((e = hLoc[0].reserve(nl)) || (e = hLoc[1].reserve(nl)))
+        if ((e = hLoc[0].reserve(nl)) || (e = hLoc[1].reserve(nl)) ||
+            (e = hLocSpare.reserve(nl)) || (e = hTimesSpare.reserve(N)))
             return cuda_status(lastError, e, "pinned host allocation");
         std::memset(hLoc[0].p, 0, nl * sizeof(double));
         std::memset(hLoc[1].p, 0, nl * sizeof(double));
@@ -470,6 +536,8 @@ struct hphc_engine {
         DeviceGuard g(rt.device);
         hLoc[0].release();
         hLoc[1].release();
+        hLocSpare.release();
+        hTimesSpare.release();
         set.release();
         dProbs.release();
         dSums.release();
@@ -817,10 +885,11 @@ int hphc_set_times_data(hphc_engine* e, const double* data, size_t length) {
     if (length != (size_t)e->N)
         return e->fail(HPHC_ERR_BAD_LENGTH, "times: length %zu != locationCount %d", length, e->N);
     size_t bad = 0;
-    if (!all_finite(data, length, &bad))
+    bool ascending = false;
+    if (!copy_checked<true>(data, e->hTimesSpare.p, length, &bad, &ascending))
         return e->fail(HPHC_ERR_NONFINITE, "times: entry %zu is not finite", bad);
-    std::memcpy(e->set.hTimes.p, data, length * sizeof(double));
-    e->set.derive_times();
+    e->set.hTimes.swap(e->hTimesSpare);
+    e->set.derive_times(ascending ? 1 : 0);
     e->dirty = true;
     e->invalidate_sums();
     return HPHC_OK;
@@ -844,6 +913,14 @@ int hphc_update_locations(hphc_engine* e, int locationIndex, const double* locat
         offset = (size_t)locationIndex * e->D;
     }
     size_t bad = 0;
+    if (locationIndex == -1) {
+        if (!copy_checked<false>(location, e->hLocSpare.p, length, &bad, nullptr))
+            return e->fail(HPHC_ERR_NONFINITE, "locations: entry %zu is not finite", bad);
+        e->hLoc[e->curLoc].swap(e->hLocSpare);
+        e->invalidate_sums();
+        e->dirty = true;
+        return HPHC_OK;
+    }
     if (!all_finite(location, length, &bad))
         return e->fail(HPHC_ERR_NONFINITE, "locations: entry %zu is not finite", bad);
     double* row = e->hLoc[e->curLoc].p + offset;
@@ -1054,6 +1131,27 @@ int hphc_set_unit_sums(hphc_engine* e, const double* deviceParts, int numParts, 
         return e->fail(HPHC_ERR_BAD_ARGUMENT,
                        "unit sums: input is not device memory of device %d", e->rt.device);
     return e->set_unit_sums(deviceParts, numParts);
+}
+
+int hphc_eval_exponentials(int device, const float* args, size_t n, float* poly,
+                           float* hardware) {
+    if (!args || !poly || !hardware || n == 0 || n > (size_t(1) << 28))
+        return HPHC_ERR_BAD_ARGUMENT;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count < 1) return HPHC_ERR_NO_DEVICE;
+    if (device < 0 || device >= count) return HPHC_ERR_BAD_ARGUMENT;
+    DeviceGuard g(device);
+    if (!g.ok) return HPHC_ERR_CUDA;
+    float* d = nullptr;
+    if (cudaMalloc(&d, 3 * n * sizeof(float)) != cudaSuccess) return HPHC_ERR_OUT_OF_MEMORY;
+    cudaError_t e = cudaMemcpy(d, args, n * sizeof(float), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = launch_eval_exponentials((int)n, d, d + n, d + 2 * n, nullptr);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(poly, d + n, n * sizeof(float), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(hardware, d + 2 * n, n * sizeof(float), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    return e == cudaSuccess ? HPHC_OK : HPHC_ERR_CUDA;
 }
 
 int hphc_inject_fault(hphc_engine* e, int stage, int count) {

@@ -468,6 +468,8 @@ int Executor::build_plan(const std::vector<SetView>& sets, const int* setOf, con
             }
         }
         sp.searchBand = (wideBands_ && s.sorted) ? 1 : 0;
+        sp.rowOrder = (fp32 && sp.symmetric) ? (r == 2 ? s.dOrder2 : r == 4 ? s.dOrder4 : nullptr)
+                                             : nullptr;
         sp.colAcc = nullptr;
         if (sp.symmetric) {
             sp.colAcc = reinterpret_cast<unsigned long long*>(colOff + 1);  // offset + 1

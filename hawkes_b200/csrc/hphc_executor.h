@@ -32,6 +32,8 @@ struct SetView {
     const double* dLoc = nullptr;      // N x D raw coordinates
     const double* dTimes = nullptr;    // N raw times
     const int32_t* dRanks = nullptr;   // dense time ranks (FP32 mode)
+    const int32_t* dOrder2 = nullptr;  // spatial row order of strips of R = 2 and 4 (FP32
+    const int32_t* dOrder4 = nullptr;  //   mode, launch_strip_order), or null
     const double* dRecF64 = nullptr;   // FP64 records (FP64 mode)
     const double* dTileMin = nullptr;  // per-tile time bounds
     const double* dTileMax = nullptr;

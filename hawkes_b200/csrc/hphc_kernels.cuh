@@ -56,7 +56,11 @@ struct PairConsts {
     // Self-excitation-only sweep: no background term is evaluated (the
     // finish takes the background sums from an earlier sweep, which depend
     // on tauX and tauT only).
-    int noB, pad;
+    int noB;
+    // FP32 software-exponential mode: factor applied to the far-tail
+    // background terms, which come from ex2.approx: 1 / (1 + its mean
+    // relative error measured on the device).
+    float farScale;
 };
 
 // Constants of the per-event finish (all FP64).
@@ -72,6 +76,8 @@ struct FinishConsts {
     double T;         // t[N-1]
     double constant;  // N (D-1) log(1/sqrt(2 pi))
     int D;
+    int plain32;      // FP32 throughout: the per-event finish in float (the reference's
+                      // single precision, src/factory.cpp:45)
 };
 
 // What param_consts needs besides the parameters: fixed per engine (mode)
@@ -79,10 +85,12 @@ struct FinishConsts {
 struct ConstsSpec {
     int precision;    // HPHC_PRECISION_* (0 = FP64)
     int D;
-    int variant;      // FP32 variant bits (2 = software exponential)
+    int variant;      // FP32 variant bits (2 = software exponential, 8 = plain FP32)
     int skip;         // tile-level underflow skip on
     int truncate;     // background tail truncation at 2^-kNegligibleLog2 (needs skip)
-    double ex2Bias;   // mean relative error of ex2.approx (hardware-exponential variant)
+    double ex2Bias;   // mean relative error of ex2.approx (FP32 modes: divided out of the
+                      // sums of the hardware-exponential variant, and of the far-tail
+                      // terms of the software-exponential one)
     int fastTail;     // far-tail tile pairs use the hardware exponential (FP32 software-
                       // exponential variant, and FP64)
     int noB;          // self-excitation-only sweep (PairConsts::noB)
@@ -114,15 +122,19 @@ constexpr double kSkipF64 = 760.0;
 
 // Background tail truncation.  Every event's background sum holds its own
 // term, B_ii = 1 unit, the largest of all its terms.  A tile pair whose
-// background terms are all at most 2^-91 units is skipped: the skipped
-// terms of one event add up to at most N 2^-91 <= 2^-60 of its sum (N <
-// 2^31), and those weighted by a squared scaled distance x (the gradient
-// sums) to at most x e^-x <= 64 2^-91 each, since x >= 91 ln 2 there.  That
-// is below FP64 rounding of the sums in both modes.  At b = 1/336 per hour
-// the cut falls at |dt| = 11.2 / b = 3774 h, against 13.3 / b for FP32
-// underflow.  The self-excitation sums have no such lower bound and keep the
-// underflow skip only.
+// background terms are all at most 2^-T units is skipped: the skipped terms
+// of one event add up to at most N 2^-T of its sum, and those weighted by a
+// squared scaled distance x (the gradient sums) to at most x e^-x <= T 2^-T
+// each, since x >= T ln 2 there.  FP64 mode: T = 91, so N 2^-91 <= 2^-60
+// (N < 2^31), below FP64 rounding of the sums; at b = 1/336 per hour the
+// cut falls at |dt| = 11.2 / b = 3774 h (FP64 underflow never cuts inside an
+// 8760 h span).  FP32 modes: T = 60, so N 2^-60 <= 2^-33 = 1.2e-10 for any
+// N the symmetric sweep holds (2^27), far below their own rounding; the cut
+// falls at |dt| = 9.1 / b = 3070 h, against 13.3 / b for FP32 underflow.
+// The self-excitation sums have no such lower bound and keep the underflow
+// skip only.
 constexpr double kNegligibleLog2 = 91.0;
+constexpr double kNegligibleLog2F32 = 60.0;
 
 // The parameter-dependent constants of one problem: every PairConsts field
 // and every FinishConsts field except T and constant (which depend on the
@@ -155,14 +167,15 @@ inline void param_consts(const double* p, const ConstsSpec& s, PairConsts& c, Fi
     }
     const double kLn2 = 0.693147180559945309417232121458176568;
     const double thr = fp32 ? kSkipF32 : kSkipF64;
-    const double thrB = s.truncate ? fmin(thr, kNegligibleLog2 * kLn2) : thr;
+    const double thrB =
+        s.truncate ? fmin(thr, (fp32 ? kNegligibleLog2F32 : kNegligibleLog2) * kLn2) : thr;
     c.skipB = (s.skip && c.cB < 0.0 && c.cA <= 0.0) ? thrB : -1.0;
     c.skipS = (s.skip && c.cW < 0.0 && c.cS <= 0.0) ? thr : -1.0;
     c.fastB = (s.fastTail && (!fp32 || (s.variant & 2)) && c.cB < 0.0 && c.cA <= 0.0)
                   ? (fp32 ? kFastTailLog2 : kFastTailLog2F64) * kLn2
                   : -1.0;
     c.noB = s.noB;
-    c.pad = 0;
+    c.farScale = (fp32 && (s.variant & 2)) ? (float)(1.0 / (1.0 + s.ex2Bias)) : 1.0f;
 
     double aD = 1.0, sigmaD = 1.0;
     for (int k = 0; k < s.D; ++k) {
@@ -184,10 +197,11 @@ inline void param_consts(const double* p, const ConstsSpec& s, PairConsts& c, Fi
         f.accScale[1] = f.accScale[4] = 1.0 / (sX * sX);  // sums of d'^2
         f.accScale[2] = 1.0 / (sT * sT);                  // sum of dt'^2
         f.accScale[5] = 1.0 / sT;                         // sum of dt'
-        if (!(s.variant & 2))  // hardware exponential: divide out its mean relative error
-            for (int q = 0; q < kNumAcc; ++q) f.accScale[q] /= 1.0 + s.ex2Bias;
+        if (!(s.variant & (2 | 8)))  // hardware exponential: divide out its mean relative
+            for (int q = 0; q < kNumAcc; ++q) f.accScale[q] /= 1.0 + s.ex2Bias;  // error
     }
     f.D = s.D;
+    f.plain32 = (fp32 && (s.variant & 8)) ? 1 : 0;
 }
 
 struct SweepGeometry {
@@ -206,14 +220,23 @@ struct SweepGeometry {
 cudaError_t launch_pack_f64(int D, int N, const double* loc, const double* times, double* rec,
                             double* tileMin, double* tileMax, cudaStream_t s);
 // Per-tile time bounds; tileChanges (nullable) receives each tile's count of
-// events whose time differs from the previous event's.
+// events whose time differs from the previous event's (floatTimes: after
+// rounding both to FP32).
 cudaError_t launch_tile_bounds(int N, const double* times, double* tileMin, double* tileMax,
-                               int* tileChanges, cudaStream_t s);
+                               int* tileChanges, cudaStream_t s, int floatTimes = 0);
 // Dense time ranks of SORTED times from the tile counts of launch_tile_bounds
 // (which it overwrites with their exclusive prefix sums): rank[j] = number of
 // k in 1..j with t_k != t_{k-1}.  Two launches.
 cudaError_t launch_sorted_ranks(int N, const double* times, int* tileChanges, int32_t* ranks,
-                                cudaStream_t s);
+                                cudaStream_t s, int floatTimes = 0);
+
+// Target-row order of the FP32 symmetric sweep with R events per thread:
+// within each full strip of 128 R events, rows sorted along a Morton curve of
+// their first two coordinates and dealt to threads in runs of R (spatial
+// neighbours share a thread); the last partial strip keeps its order.  One
+// or two launches.
+cudaError_t launch_strip_order(int D, int N, int R, const double* loc, int32_t* order,
+                               cudaStream_t s);
 
 // Pair sweep: fills partials[chunk][6][Npad] with unit pair sums.  R is the
 // number of target events per thread (strip = kSweepThreads * R events).
@@ -237,6 +260,11 @@ cudaError_t launch_final(int nBlocks, const double* blockSums, const FinishConst
 // Calibration of the FP32 exponential: writes ceil(n / kFinishThreads) CTA
 // sums of (ex2.approx(x) / 2^x - 1) for n arguments spread over [-16, 0).
 cudaError_t launch_ex2_bias(int n, double* blockSums, cudaStream_t s);
+
+// Test of the FP32 sweep's exponentials: poly[k] = 2^-s[k] by the software
+// exponential, hw[k] = ex2.approx.ftz(-s[k]); s[k] >= 0, device arrays of n.
+cudaError_t launch_eval_exponentials(int n, const float* s, float* poly, float* hw,
+                                     cudaStream_t st);
 
 // Number of finish CTAs for N events.
 inline int finish_blocks(int N) { return (N + kFinishThreads - 1) / kFinishThreads; }
@@ -282,6 +310,10 @@ struct SweepProblem {
     // for any sigma and omega, sorted times): the sweep finds that tile by
     // bisection on the tile time bounds instead of scanning to it.
     int searchBand, pad[3];
+    // FP32 sweep: event of row r of thread t of a full strip, at
+    // [stripBase + r * 128 + t] (launch_strip_order for the sweep's R), or
+    // null for the identity order.
+    const int32_t* rowOrder;
     PairConsts c;
 };
 

@@ -17,7 +17,14 @@
 // is only a host-side stand-in, so its device address is looked up once per
 // device with cudaGetSymbolAddress (with that device current) and passed to
 // the kernels.  That lookup happens in the first call on each device, which
-// is why the first call should come before any stream capture.
+// is why the first call should come before any stream capture.  A device
+// whose context was destroyed (cudaDeviceReset) gets a new context and a
+// new copy of the array on its next use, so the address is cached together
+// with the context's unique id and looked up again when that id changes.
+//
+// Device inputs are used as given: they are not checked for non-finite
+// values or for ordering (times need not be sorted; T is t[N-1], as in the
+// reference).  A NaN or infinity in them gives a non-finite result.
 //
 // Sharing: all calls in the process use the same array.  Every scratch word a
 // call reads is written earlier in the same call, so nothing has to start at
@@ -48,16 +55,48 @@ static __device__ __align__(256) double g_hphc_static_scratch[kScratchDoubles];
 
 std::mutex gScratchMutex;
 double* gScratchAddress[kMaxDevices] = {};
+unsigned long long gScratchContext[kMaxDevices] = {};
 
-// Device address of the static scratch on the current device (looked up once).
+// Unique id of the current context (cuCtxGetCurrent + cuCtxGetId through the
+// runtime's driver entry points, so the library needs no link against the
+// driver library); 0 if it cannot be read.  Called with gScratchMutex held.
+unsigned long long current_context_id() {
+    using GetCurrent = int (*)(void**);
+    using GetId = int (*)(void*, unsigned long long*);
+    static GetCurrent getCurrent = nullptr;
+    static GetId getId = nullptr;
+    static bool looked = false;
+    if (!looked) {
+        looked = true;
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            getCurrent = reinterpret_cast<GetCurrent>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            getId = reinterpret_cast<GetId>(f);
+    }
+    void* ctx = nullptr;
+    unsigned long long id = 0;
+    if (!getCurrent || !getId || getCurrent(&ctx) != 0 || !ctx || getId(ctx, &id) != 0) return 0;
+    return id;
+}
+
+// Device address of the static scratch on the current device: looked up on
+// the first call on the device, and again after its context was recreated.
 cudaError_t static_scratch_address(int device, double** out) {
     std::lock_guard<std::mutex> lock(gScratchMutex);
     if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
-    if (!gScratchAddress[device]) {
+    const unsigned long long ctx = current_context_id();
+    if (!gScratchAddress[device] || ctx == 0 || ctx != gScratchContext[device]) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_hphc_static_scratch);
         if (e != cudaSuccess) return e;
         gScratchAddress[device] = static_cast<double*>(p);
+        gScratchContext[device] = ctx;
     }
     *out = gScratchAddress[device];
     return cudaSuccess;
@@ -152,34 +191,24 @@ extern "C" int hphc_loglik_grad_fp64_static(int embeddingDimension, int location
         cudaStreamSynchronize(s) != cudaSuccess)
         return HPHC_ERR_CUDA;
 
-    const double sigma = params[0], a = params[1], b = params[2], omega = params[3],
-                 theta = params[4], mu0 = params[5];
+    // The same constants as the engine's FP64 mode (hphc::param_consts),
+    // with the tile-level underflow skip only: no tail truncation, no far
+    // tail on the hardware exponential.
+    ConstsSpec spec{};
+    spec.precision = 0;
+    spec.D = D;
+    spec.variant = 0;
+    spec.skip = 1;
+    spec.truncate = 0;
+    spec.ex2Bias = 0.0;
+    spec.fastTail = 0;
+    spec.noB = 0;
     PairConsts c{};
-    c.cA = -0.5 * a * a;
-    c.cB = -0.5 * b * b;
-    c.cS = -0.5 * sigma * sigma;
-    c.cW = -omega;
-    const double kSkip = 760.0;  // FP64 exp(x) is +0 below -745.2
-    c.skipB = (c.cB < 0.0) ? kSkip : -1.0;
-    c.skipS = (c.cW < 0.0) ? kSkip : -1.0;
-
-    const double kInvSqrt2Pi = 0.398942280401432677939946059934;
-    const double kTwoPi = 6.28318530717958647692528676655900577;
     FinishConsts f{};
-    f.sigma = sigma;
-    f.a = a;
-    f.b = b;
-    f.omega = omega;
-    f.theta = theta;
-    f.mu0 = mu0;
-    f.bgScale = std::pow(a, D) * b / kTwoPi;
-    f.seScale = omega * std::pow(sigma, D) * kInvSqrt2Pi;
-    f.prefB = mu0 * f.bgScale;
-    f.prefS = theta * f.seScale;
-    for (int q = 0; q < kNumAcc; ++q) f.accScale[q] = 1.0;
+    param_consts(params, spec, c, f);
+    const double kInvSqrt2Pi = 0.398942280401432677939946059934;
     f.T = T;
     f.constant = (double)(N * (D - 1)) * std::log(kInvSqrt2Pi);
-    f.D = D;
 
     double* rec = scratch + plan.rec;
     double* tmin = scratch + plan.tmin;

@@ -66,6 +66,7 @@ PATH_SELF_EXCITATION = 3
 
 PRECISION_FP64 = 0
 PRECISION_FP32_COMP = 1
+PRECISION_FP32 = 2  # FP32 throughout: the reference's single precision (FLOAT alone)
 
 # Parameter order of NewHawkes::setParameters (src/NewHawkes.hpp:331-339).
 PARAMETER_NAMES = ("sigmaXprec", "tauXprec", "tauTprec", "omega", "theta", "mu0")
@@ -380,7 +381,9 @@ def factory(embeddingDimension: int, locationCount: int, flags: int, device: int
     """``hph::factory`` (src/factory.cpp:32) restricted to its GPU slot.
 
     ``OPENCL`` or ``CUDA`` in flags selects the CUDA engine; ``FLOAT`` (the
-    reference's single-precision request) selects the FP32-compensated mode.
+    reference's single-precision request) selects FP32 throughout, as the
+    reference's float engine; ``COMPENSATED`` selects the FP32-compensated mode
+    (FP32 pair terms, compensated sums, FP64 reductions).
     ``threads`` is accepted for signature compatibility and ignored.
     """
     if not flags & (OPENCL | CUDA):
@@ -396,19 +399,22 @@ class Engine(dict):
 
 
 def createEngine(embeddingDimension: int, locationCount: int, tbb: int = 0, simd: int = 0,
-                 gpu: int = 1, single: bool = False) -> Engine:
+                 gpu: int = 1, single: bool = False, compensated: bool = False) -> Engine:
     """``createEngine`` (src/hpHawkes.cpp:59-109) with the GPU path selected.
 
     ``gpu`` is the device number as in the R glue (``deviceNumber = gpu``,
     src/hpHawkes.cpp:68); out-of-range numbers fall back to device 0 as the
     OpenCL engine falls back to the default device.  ``single`` selects the
-    FP32-compensated mode.
+    reference's single precision (FP32 throughout); ``compensated`` (not in
+    the R glue) the FP32-compensated mode.
     """
     if gpu <= 0:
         raise HawkesError(5, "createEngine: the CUDA engine needs gpu > 0")
     flags = OPENCL | CUDA
     if single:
         flags |= FLOAT
+    if compensated:
+        flags |= COMPENSATED
     eng = CudaHawkes(embeddingDimension, locationCount, flags, gpu)
     return Engine(engine=eng, embeddingDimension=embeddingDimension,
                   locationCount=locationCount, timesInitialized=False,

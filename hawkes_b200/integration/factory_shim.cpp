@@ -7,8 +7,9 @@
 // :67-72).  Linking this file instead of src/backend/opencl/instantiate.cpp
 // defines those two constructors to build hph::CudaHawkes, so the reference's
 // factory, CLI and R entry points reach the CUDA engine without a source change.
-// The FLOAT flag (single precision, src/factory.cpp:34) selects the
-// FP32-compensated mode.
+// The FLOAT flag (single precision, src/factory.cpp:34) selects FP32
+// throughout, as the reference's float engine; a caller that wants the
+// FP32-compensated mode adds HPHC_FLAG_COMPENSATED to the flags.
 #include "hawkes_b200/CudaHawkes.hpp"
 
 namespace hph {

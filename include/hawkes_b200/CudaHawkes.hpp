@@ -35,7 +35,9 @@ public:
         int precision = 0;
         hphc_get_precision(engine, &precision);
         std::cerr << "CUDA (sm_100a), "
-                  << (precision == HPHC_PRECISION_FP64 ? "DOUBLE" : "SINGLE-COMPENSATED")
+                  << (precision == HPHC_PRECISION_FP64        ? "DOUBLE"
+                      : precision == HPHC_PRECISION_FP32_COMP ? "SINGLE-COMPENSATED"
+                                                              : "SINGLE")
                   << std::endl;
     }
 

@@ -50,7 +50,9 @@ extern "C" {
 #define HPHC_ERR_SCRATCH_TOO_SMALL 11 /* a problem needs more scratch than provided    */
 
 /* ---- flags: bit-compatible with hph::Flags (src/flags.h:6-13) ----------- */
-#define HPHC_FLAG_FLOAT (1L << 2)     /* single precision: FP32-compensated pair math */
+#define HPHC_FLAG_FLOAT (1L << 2)     /* single precision: FP32 throughout, as the
+                                         reference's float engine (with COMPENSATED:
+                                         the FP32-compensated mode)                  */
 #define HPHC_FLAG_TBB (1L << 3)       /* accepted and ignored (CPU threading flag)    */
 #define HPHC_FLAG_OPENCL (1L << 4)    /* accepted: the GPU engine slot                */
 #define HPHC_FLAG_SSE (1L << 5)       /* accepted and ignored                         */
@@ -84,11 +86,11 @@ extern "C" {
                                                 2^-60 (FP64 mode) of an event's own term take
                                                 those terms from ex2.approx) */
 #define HPHC_FLAG_NO_TAIL_TRUNCATION (1L << 16) /* skip background tile pairs only where
-                                                every term underflows (by default, in both
-                                                modes, tile pairs whose background terms are
-                                                all below 2^-91 of an event's own term are
-                                                skipped: together under 2^-60 of any
-                                                event's sums) */
+                                                every term underflows (by default tile pairs
+                                                whose background terms are all below 2^-91
+                                                (FP64) or 2^-60 (FP32 modes) of an event's
+                                                own term are skipped: together under 2^-60
+                                                and 2^-33 of any event's sums) */
 
 /* How the last evaluation was computed (hphc_get_last_evaluation_path). */
 #define HPHC_PATH_SWEEP 0        /* the O(N^2) pair sweep                             */
@@ -100,6 +102,9 @@ extern "C" {
 /* Precision modes reported by hphc_get_precision(). */
 #define HPHC_PRECISION_FP64 0          /* plain FP64 pair terms and reductions           */
 #define HPHC_PRECISION_FP32_COMP 1     /* FP32 pair terms, compensated; FP64 reductions  */
+#define HPHC_PRECISION_FP32 2          /* FP32 throughout (the reference's float engine):
+                                          pair terms, plain sums, log and CDF in float;
+                                          event totals FP64 and fixed-order            */
 
 typedef struct hphc_engine hphc_engine;
 
@@ -109,8 +114,10 @@ typedef struct hphc_engine hphc_engine;
  * Create an engine for locationCount events in embeddingDimension (1..8)
  * spatial dimensions.  Replaces hph::factory (src/factory.cpp:32) for the GPU
  * slot and the OpenCLHawkes constructor (src/backend/opencl/instantiate.cpp:15-52).
- * flags: HPHC_FLAG_FLOAT or HPHC_FLAG_COMPENSATED select the FP32-compensated
- * mode, otherwise plain FP64.  device: CUDA device ordinal; a value < 0 or
+ * flags: HPHC_FLAG_COMPENSATED selects the FP32-compensated mode (FP32 pair
+ * terms, compensated sums, FP64 reductions; with or without HPHC_FLAG_FLOAT);
+ * HPHC_FLAG_FLOAT alone the plain FP32 mode, the reference's single precision
+ * (src/factory.cpp:34, :45); otherwise plain FP64.  device: CUDA device ordinal; a value < 0 or
  * beyond the device count selects device 0, as the OpenCL engine falls back to
  * the default device (src/backend/opencl/OpenCLHawkes.hpp:88-92).
  */
@@ -302,10 +309,14 @@ int hphc_sampler_get_state(const hphc_sampler* sampler, double* params, double* 
  * gradient, [7] zero.  The call runs on `stream` (a cudaStream_t, or null
  * for the default stream) and returns when the result is written.
  *
- * The first call on a device looks up the static array's device address
- * (cudaGetSymbolAddress); make that first call before any stream capture.
- * Every call shares the one array: calls that overlap on the GPU (other
- * streams or threads) race and corrupt each other's results. */
+ * The first call on a device does a one-time set-up: it looks up the static
+ * array's device address (cudaGetSymbolAddress), and looks it up again after
+ * the device's context was destroyed and recreated (cudaDeviceReset).  Make
+ * that first call before any stream capture begins.  Device inputs are not
+ * checked: a NaN or infinity in them gives a non-finite result; times need
+ * not be sorted (T = t[N-1], as in the reference).  Every call shares the one
+ * array: calls that overlap on the GPU (other streams or threads) race and
+ * corrupt each other's results. */
 int hphc_loglik_grad_fp64_static(int embeddingDimension, int locationCount,
                                  const double* deviceLocations, const double* deviceTimes,
                                  const double* params, double* deviceOut, void* stream);
@@ -351,6 +362,16 @@ int hphc_set_unit_sums(hphc_engine* engine, const double* deviceParts, int numPa
 int hphc_inject_fault(hphc_engine* engine, int stage, int count);
 
 /* ---- introspection and device-resident timing --------------------------- */
+
+/* No reference counterpart (the reference's exponentials are libm's).  The
+ * two exponentials of the FP32 modes evaluated on `device` for n host
+ * arguments s >= 0: poly[k] = 2^-s[k] by the software exponential (Cody-Waite
+ * reduction, degree-7 polynomial, exact power of two; near terms), and
+ * hardware[k] = ex2.approx.ftz(-s[k]) (far-tail background terms).  For
+ * testing their error bounds against FP64.  Allocates device memory;
+ * synchronous; n at most 2^28. */
+int hphc_eval_exponentials(int device, const float* args, size_t n, float* poly,
+                           float* hardware);
 
 /* Precision mode in use (HPHC_PRECISION_*). */
 int hphc_get_precision(hphc_engine* engine, int* out);
@@ -399,8 +420,8 @@ int hphc_get_last_evaluation_path(hphc_engine* engine, int* path);
  * sweep evaluated.  Of the 2 N^2 possible terms the rest were skipped at tile
  * level: the non-causal half of the self-excitation sum, tile pairs whose
  * terms all underflow to exactly zero in the working precision, and (tail
- * truncation) background tile pairs whose terms are all below 2^-91 of an
- * event's own term. */
+ * truncation) background tile pairs whose terms are all below 2^-91 (FP64) or
+ * 2^-60 (FP32 modes) of an event's own term. */
 int hphc_get_last_launch_stats(hphc_engine* engine, int* kernelLaunches,
                                double* backgroundTerms, double* selfExciteTerms);
 

@@ -1,6 +1,6 @@
-"""Fit the polynomial used by the FP32 software exponential in hphc_kernels.cu.
+"""Fit the polynomial used by the FP32 software exponential (hawkes_b200/csrc/hphc_sweep.cuh).
 
-    python hawkes_b200/csrc/fit_exp2.py [degree]
+    python tests/fit_exp2.py [degree]
 
 2^x is evaluated as 2^n * p(f) with n = round(x), f = x - n in [-1/2, 1/2]
 (Cody-Waite range reduction, W. J. Cody and W. Waite, "Software Manual for the
@@ -55,7 +55,7 @@ def horner32(c32, f32):
 
 
 def main():
-    deg = int(sys.argv[1]) if len(sys.argv) > 1 else 6
+    deg = int(sys.argv[1]) if len(sys.argv) > 1 else 7
     c32 = fit_fp32(deg).astype(np.float32)
     x = np.linspace(-0.5, 0.5, 200001)
     exact = np.exp2(x)

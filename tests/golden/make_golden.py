@@ -1,11 +1,15 @@
 """Generate the golden parity fixtures in tests/golden/ (run in a container
 that has the reference sources; the fixtures are committed).
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py --reference <reference checkout>
+
+(or HAWKES_REF set to the checkout).
 
 Every expected log-likelihood and probability vector comes from the reference
 hpHawkes CPU engine itself (src/NewHawkes.hpp, serial DOUBLE path), compiled
-from its sources by oracle/Makefile into oracle/_ref/libhawkes_ref.so.  The
+from its sources by oracle/Makefile into oracle/_ref/libhawkes_ref.so; the
+``ref_float_*`` fields come from the same engine's single-precision path
+(FLOAT, src/factory.cpp:45: every pair term, sum, log and CDF in float).  The
 reference has no live gradient; expected gradients are the oracle's analytic
 gradient (oracle/hawkes_oracle.c), stored together with central finite
 differences of the reference engine's log-likelihood that pin it.
@@ -83,8 +87,8 @@ def read_rdata_columns(path: str) -> dict:
     return dict(zip(names, cols))
 
 
-def reference_outputs(loc, t, p):
-    eng = oracle.RefEngine(loc.shape[1], loc.shape[0], threads=0)
+def reference_outputs(loc, t, p, single=False):
+    eng = oracle.RefEngine(loc.shape[1], loc.shape[0], threads=0, single=single)
     eng.set_data(loc, t)
     eng.set_parameters(p)
     ll = eng.loglik()
@@ -117,10 +121,12 @@ def case(name, loc, t, p, store, fd=True):
     t = np.ascontiguousarray(t, dtype=np.float64)
     p = np.asarray(p, dtype=np.float64)
     ll, pr, variant = reference_outputs(loc, t, p)
+    ll32, pr32, _ = reference_outputs(loc, t, p, single=True)
     o = oracle.oracle_eval(loc, t, p, threads=8)
     entry = {
         "loc": loc, "t": t, "params": p,
         "ref_loglik": np.float64(ll), "ref_probs": pr,
+        "ref_float_loglik": np.float64(ll32), "ref_float_probs": pr32,
         "oracle_grad": o["grad"], "grad_scale": o["grad_scale"],
         "grad_term_scale": o["grad_term_scale"],
     }
@@ -141,8 +147,11 @@ def save(store, fname):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("HAWKES_REF", ""),
+                    help="the reference checkout (its src/ and data/ are read)")
     args = ap.parse_args()
+    if not args.reference:
+        ap.error("--reference (or HAWKES_REF) is required")
     oracle.build(os.path.join(args.reference, "src"))
 
     synth = {}

@@ -10,15 +10,19 @@ twice in a row on different event sets (the shared static scratch must not
 carry anything from one call into the next) and once more on the first set,
 and compares every result with the engine entry point
 (hphc_get_log_likelihood_and_gradient, FP64 mode) within the FP64 tolerance
-of the parity tests.  This file is collected last so that a failing run that
-stops at the first failure has already run every other test.
+of the parity tests, and the first one also with the oracle.  A set with
+unsorted and tied times checks the same against the engine.  This file is
+collected last so that a failing run that stops at the first failure has
+already run every other test.
 """
 import ctypes
+import os
 
 import numpy as np
 import pytest
 
 import hawkes_b200 as hb
+import oracle
 from hawkes_b200 import _native, workloads
 
 pytestmark = pytest.mark.gpu
@@ -70,6 +74,21 @@ def test_static_scratch_entry_point_matches_engine():
     close(second_b, engine_result(loc_b, t_b, p_b))
     again_a = static_result(torch, loc_a, t_a, p_a)
     assert again_a[0] == first_a[0] and np.array_equal(again_a[1], first_a[1])
+
+    o = oracle.oracle_eval(loc_a, t_a, p_a, threads=max(1, os.cpu_count() or 1))
+    assert abs(first_a[0] - o["loglik"]) <= 1e-10 * abs(o["loglik"])
+    assert np.all(np.abs(first_a[1] - o["grad"]) <= 1e-10 * o["grad_scale"])
+
+
+def test_static_scratch_unsorted_and_tied_times():
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(23)
+    loc = rng.uniform(0.0, 20.0, size=(1500, 2))
+    t = rng.integers(0, 300, size=1500).astype(np.float64) * 5.0  # many exact ties
+    m = int(np.argmax(t))
+    t[m], t[-1] = t[-1], t[m]  # unsorted, the latest time last (T = t[N-1])
+    p = workloads.BASE_PARAMS * np.array([0.8, 1.1, 1.4, 0.9, 1.2, 1.0])
+    close(static_result(torch, loc, t, p), engine_result(loc, t, p))
 
 
 def test_static_scratch_rejects_oversized_problems():
