@@ -61,6 +61,13 @@ struct PairConsts {
     // background terms, which come from ex2.approx: 1 / (1 + its mean
     // relative error measured on the device).
     float farScale;
+    // FP32-compensated mode: the value each row sum's hi part starts from, a
+    // power of two at least as large as any single unit term of that sum
+    // (B_u, S_u <= 1; B_u d'^2, B_u dt'^2 <= 1/(e ln 2); S_u d'^2 <=
+    // 1/(e ln 2 |kS|); S_u dt' <= 1/(e ln 2 |kW|)), and at least 1.  Every
+    // addition to hi then has |hi| >= |term|, so its Fast2Sum error is exact
+    // whatever order the terms come in.  Zero in the other modes.
+    float rowOffset[kNumAcc];
 };
 
 // Constants of the per-event finish (all FP64).
@@ -176,6 +183,20 @@ inline void param_consts(const double* p, const ConstsSpec& s, PairConsts& c, Fi
                   : -1.0;
     c.noB = s.noB;
     c.farScale = (fp32 && (s.variant & 2)) ? (float)(1.0 / (1.0 + s.ex2Bias)) : 1.0f;
+    for (int q = 0; q < kNumAcc; ++q) c.rowOffset[q] = 0.0f;
+    if (fp32 && !(s.variant & 8)) {
+        const double kMaxUe = 0.53071497680680994;  // max of u 2^-u over u >= 0: 1/(e ln 2)
+        const double kS = fabs((double)c.fSh + (double)c.fSl);
+        const double kW = fabs((double)c.fWh + (double)c.fWl);
+        const double bound[kNumAcc] = {1.0, kMaxUe, kMaxUe, 1.0,
+                                       kS > 0.0 ? kMaxUe / kS : 1e30,
+                                       kW > 0.0 ? kMaxUe / kW : 1e30};
+        for (int q = 0; q < kNumAcc; ++q) {
+            double h = 1.0;
+            while (h < bound[q] && h < 0x1p100) h *= 2.0;
+            c.rowOffset[q] = (float)h;
+        }
+    }
 
     double aD = 1.0, sigmaD = 1.0;
     for (int k = 0; k < s.D; ++k) {

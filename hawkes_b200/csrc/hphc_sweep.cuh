@@ -611,8 +611,17 @@ __device__ __forceinline__ float2 self_dt2(const StagedTile<D>& t, int p, const 
 // of the running sum is rounded away entirely, so sums of many small terms
 // come out low (measured at N = 100k: about -2.5e-9 relative on every
 // background sum, which the cancelling d/d tauX and d/d tauT gradient
-// components amplify about 80-fold).  The row value is hi + lo, formed in
-// FP64 when the work item writes its partial sums.
+// components amplify about 80-fold).
+//
+// hi starts from PairConsts::rowOffset, a power of two no smaller than any
+// single term of the sum, so |hi| >= |x| holds at every addition and each
+// error is exact whatever order the terms come in (starting from zero, a
+// term larger than the sum so far -- the nearest neighbour arriving late in
+// a chunk -- would round with an error Fast2Sum does not see: ~1e-8 of an
+// event's sum, moving with the chunk bounds).  Terms far below the offset
+// pass to lo whole, where they add up in plain FP32 at their own scale.
+// The row value (hi - offset) + lo is formed in FP64 when the work item
+// writes its partial sums (hi - offset is exact there: two FP32 values).
 //
 // Far-tail background terms (each at most 2^-12 of the event's own term, see
 // kFastTailLog2) are added to lo directly: lo then carries them and the
@@ -625,11 +634,14 @@ struct RowSums {
 };
 
 template <int R>
-__device__ __forceinline__ void zero_rows(RowSums<R>& a) {
+__device__ __forceinline__ void start_rows(RowSums<R>& a, const PairConsts& c) {
 #pragma unroll
     for (int r = 0; r < R; ++r)
 #pragma unroll
-        for (int q = 0; q < kNumAcc; ++q) a.hi[r][q] = a.lo[r][q] = make_float2(0.0f, 0.0f);
+        for (int q = 0; q < kNumAcc; ++q) {
+            a.hi[r][q] = make_float2(c.rowOffset[q], c.rowOffset[q]);
+            a.lo[r][q] = make_float2(0.0f, 0.0f);
+        }
 }
 
 // hi += x with the rounding error added to lo.
@@ -906,7 +918,7 @@ __device__ __forceinline__ void f32c_item(const float* __restrict__ rec,
         }
     }
     RowSums<R> acc;
-    zero_rows<R>(acc);
+    start_rows<R>(acc, c);
 
     for (int jt = jt0; jt < jt1; ++jt) {
         TileMode m = tile_mode(tminI, tmaxI, tileMin[jt], tileMax[jt], c);
@@ -996,7 +1008,8 @@ __device__ __forceinline__ void f32c_item(const float* __restrict__ rec,
                 // the kept sums: they are neither written nor read
                 if (q >= 3 || !c.noB)
                     partials[((size_t)slot * kNumAcc + q) * Npad + i] =
-                        ((double)acc.hi[r][q].x + (double)acc.hi[r][q].y) +
+                        (((double)acc.hi[r][q].x - (double)c.rowOffset[q]) +
+                         ((double)acc.hi[r][q].y - (double)c.rowOffset[q])) +
                         ((double)acc.lo[r][q].x + (double)acc.lo[r][q].y);
         }
     }

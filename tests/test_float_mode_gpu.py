@@ -15,8 +15,11 @@ Bars (the fixtures' ref_float_* fields come from the reference float engine;
 ref_* from its double engine):
   synthetic cases   log-likelihood within 5e-6 relative of both the reference
                     float and double results; P_i within 2e-3 absolute of the
-                    float engine's; gradient within 1e-4 of the oracle's
-                    term-level scale.
+                    float engine's; gradient within 1e-3 of the oracle's
+                    term-level scale (times of up to 8760 h rounded to float
+                    are off by up to 2^-11 h, which moves each
+                    self-excitation term by up to omega * 2^-11 ~ 5e-4
+                    relative at omega = 1).
   dcData            log-likelihood within 5e-6 relative of the reference float
                     engine (which is itself ~3e-4 from double there) and P_i
                     within 2e-3 of the float engine's.
@@ -61,7 +64,7 @@ def test_float_mode_synthetic(golden_synthetic):
         assert r32 <= 5e-6 and r64 <= 5e-6, name
         assert p32 <= 2e-3, name
         o_scale = c["grad_term_scale"]
-        assert np.all(np.abs(g - c["oracle_grad"]) <= 1e-4 * o_scale + 1e-12), name
+        assert np.all(np.abs(g - c["oracle_grad"]) <= 1e-3 * o_scale + 1e-12), name
 
 
 def test_float_mode_dcdata(golden_dcdata):

@@ -149,9 +149,15 @@ def test_symmetric_sweep_halves_background_work(sym, ordered):
 
 
 @pytest.mark.parametrize("flags", MODES, ids=IDS)
-def test_underflow_skip_is_bit_exact(flags):
+def test_underflow_skip_is_bit_exact_in_fp64(flags):
     # Tile pairs whose terms all underflow are skipped; evaluating them anyway
-    # must give identical bits.
+    # must give identical bits in FP64.  In the FP32 modes a tile pair that
+    # carries self-excitation terms takes its coordinate differences from hi +
+    # lo parts (background-only pairs from hi parts, each event's coordinates
+    # then off by up to half an FP32 ulp): evaluating the underflowed
+    # self-excitation pairs gives their background terms the exact
+    # coordinates.  Measured: 7e-12 on the log-likelihood, 6e-8 on the
+    # strongly cancelling d/d tauT component, 7e-8 on P_i.
     loc, t = workloads.uniform(20000, seed=7)
     p = workloads.BASE_PARAMS
     with engine(loc, t, p, flags | hb.NO_TAIL_TRUNCATION) as a, \
@@ -164,7 +170,12 @@ def test_underflow_skip_is_bit_exact(flags):
         _, nba, nsa = a.lastLaunchStats()
         _, nbb, nsb = b.lastLaunchStats()
         pa, pb = a.getProbsSelfExcite(), b.getProbsSelfExcite()
-    assert la == lb and np.array_equal(ga, gb) and np.array_equal(pa, pb)
+    if not flags & hb.COMPENSATED:
+        assert la == lb and np.array_equal(ga, gb) and np.array_equal(pa, pb)
+    else:
+        assert abs(la - lb) <= 5e-11 * abs(lb)
+        assert np.all(np.abs(ga - gb) <= 2e-7 * np.abs(gb) + 1e-12)
+        assert np.max(np.abs(pa - pb)) <= 2e-7
     assert nba + nsa < nbb + nsb  # the skip did remove work
     assert nbb == 20000.0 ** 2  # without it every background term is evaluated
 

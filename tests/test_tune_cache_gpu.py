@@ -55,4 +55,6 @@ def test_tuned_shape_is_written_and_read_back(tmp_path):
     cache.write_text("not json\n" + json.dumps(other) + "\n" + json.dumps(edited) + "\n")
     third = _run(cache)
     assert third["shape"] == [line["R"], 1]
-    assert abs(third["ll"] - first["ll"]) <= 1e-12 * abs(first["ll"])
+    # other j-chunk bounds: the FP32-compensated sums restart per chunk with
+    # exact errors, so the log-likelihood moves by ~1e-15 relative
+    assert abs(third["ll"] - first["ll"]) <= 1e-13 * abs(first["ll"])
