@@ -67,6 +67,13 @@ L2_FLUSH_BYTES = 256 << 20
 # equivalent and can exceed the pipe's peak.
 FP32_PER_PAIR_EVAL, EX2_PER_PAIR_EVAL = 13.5, 1.5
 FP32_PER_B, FP32_PER_COL, FP32_PER_S = 11.0, 3.0, 5.0
+# The FP32-compensated algorithm adds to that count the work its precision
+# pattern requires: every near background term (a tile pair not in the far
+# tail) and every self-excitation term takes its time difference from hi and
+# lo parts (+2) and enters its three sums by Fast2Sum (+3 each, +9); far-tail
+# background terms (each at most 2^-12 of the event's own term) and the
+# symmetric column adds keep the plain count.
+FP32C_PER_NEAR_B, FP32C_PER_S = FP32_PER_B + 11.0, FP32_PER_S + 11.0
 FP32_LANES_PER_SM = 128
 MUFU_LANES_PER_SM = 16
 
@@ -427,6 +434,35 @@ def make_workload(name, n):
     raise ValueError(name)
 
 
+def far_tail_share(t, tau_t, R, tile=128, threads=128):
+    """Share of the symmetric FP32 sweep's background exponentials that fall
+    in far-tail tile pairs, from the tile-pair decisions on sorted times:
+    a strip of R tiles meets every tile up to its own last one; a pair is
+    skipped when every background term is below 2^-60 (tail truncation), far
+    when below 2^-12 (log2 exponent -(b dt)^2 log2(e) / 2 over min |dt|)."""
+    t = np.asarray(t, dtype=np.float64)
+    n = len(t)
+    nt = (n + tile - 1) // tile
+    pad = nt * tile - n
+    tp = np.concatenate([t, np.full(pad, np.nan)]).reshape(nt, tile)
+    lo, hi = np.nanmin(tp, 1), np.nanmax(tp, 1)
+    cnt = np.minimum(tile, n - np.arange(nt) * tile).astype(np.float64)
+    k = 0.5 * tau_t * tau_t * math.log2(math.e)  # log2 exponent per squared hour
+    near = far = 0.0
+    for s0 in range(0, nt, R):
+        s1 = min(s0 + R, nt)
+        slo, shi = lo[s0:s1].min(), hi[s0:s1].max()
+        rows = cnt[s0:s1].sum()
+        j = np.arange(s1)
+        gap = np.maximum(0.0, np.maximum(slo - hi[j], lo[j] - shi))
+        e2 = k * gap * gap
+        w = rows * cnt[j]
+        keep = e2 < 60.0
+        far += float(np.sum(w[keep & (e2 >= 12.0)]))
+        near += float(np.sum(w[keep & (e2 < 12.0)]))
+    return far / max(near + far, 1.0)
+
+
 def oracle_accuracy(res32, res64, n):
     """Errors of both arms against the committed oracle fixture of the
     headline events (tests/golden/headline_n100k.npz): log-likelihood
@@ -525,8 +561,17 @@ def ours_arm(args):
     sweep_mean = statistics.mean(sweep32)
     # the roofline counts the terms the launch evaluated; "effective" counts
     # the brute-force work (every ordered pair) the launch stands for
-    inst = FP32_PER_B * nev + FP32_PER_COL * (nb - nev) + FP32_PER_S * ns
+    inst_plain = FP32_PER_B * nev + FP32_PER_COL * (nb - nev) + FP32_PER_S * ns
+    far = (far_tail_share(w["t"], w["params"][2], shape32[0])
+           if w["kind"] == "single" and shape32 else 1.0)
+    inst = (FP32C_PER_NEAR_B * (1.0 - far) * nev + FP32_PER_B * far * nev +
+            FP32_PER_COL * (nb - nev) + FP32C_PER_S * ns)
     achieved = inst / (sweep_mean / 1e3) / 1e12
+    ncu = None
+    npath = os.path.join(ROOT, "profiles", "sweep_pipes.json")
+    if os.path.exists(npath):
+        with open(npath) as f:
+            ncu = json.load(f).get(f"fp32c_{args.workload}")
     achieved_ex2 = (nev + ns) / (sweep_mean / 1e3) / 1e12
     effective = FP32_PER_PAIR_EVAL * pairs / (sweep_mean / 1e3) / 1e12
     traffic = None
@@ -577,12 +622,22 @@ def ours_arm(args):
         "roofline": {"bound": "fp32", "kernel": kernel,
                      "achieved": achieved, "peak": peak_inst, "unit": "Tinst/s",
                      "frac": achieved / peak_inst, "traffic": traffic,
-                     "count": "FP32 instructions (FMA = 1) of the terms this launch evaluated: "
-                              f"{FP32_PER_B:g} per background exponential, {FP32_PER_COL:g} per "
-                              "background pair also added to the earlier event's sums, "
-                              f"{FP32_PER_S:g} per self-excitation term; over the mean "
-                              "CUDA-event duration of the sweep kernel",
+                     "count": "FP32 instructions (FMA = 1) of the compensated algorithm on the "
+                              "terms this launch evaluated: "
+                              f"{FP32C_PER_NEAR_B:g} per near background exponential (hi/lo time "
+                              "difference, three Fast2Sum additions), "
+                              f"{FP32_PER_B:g} per far-tail one ({far:.3f} of them), "
+                              f"{FP32_PER_COL:g} per background pair also added to the earlier "
+                              f"event's sums, {FP32C_PER_S:g} per self-excitation term; over the "
+                              "mean CUDA-event duration of the sweep kernel",
                      "instructions_per_launch": inst,
+                     "plain_count": {"instructions_per_launch": inst_plain,
+                                     "frac": inst_plain / (sweep_mean / 1e3) / 1e12 / peak_inst,
+                                     "count": f"without the compensation: {FP32_PER_B:g} per "
+                                              f"background exponential, {FP32_PER_S:g} per "
+                                              "self-excitation term"},
+                     "far_tail_share": far,
+                     "ncu": ncu,
                      "peak_source": f"{sm_count} SMs x 128 FP32 lanes x {max_mhz:.0f} MHz "
                                     f"(sm_max_mhz, {peak_src})",
                      "ex2": {"achieved": achieved_ex2, "peak": peak_ex2, "unit": "Tex2/s",
