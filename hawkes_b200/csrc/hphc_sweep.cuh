@@ -868,6 +868,23 @@ __device__ __forceinline__ void tile_sym_f32(const StagedTile<D>& t, const Rows2
     }
 }
 
+// One FP32 record (S floats, S a multiple of 4, rows 16-byte aligned) by
+// coalesced 16-byte loads: consecutive threads read consecutive records.
+template <int S>
+__device__ __forceinline__ void load_record_f32(const float* __restrict__ rec, int i,
+                                                float (&out)[S]) {
+    static_assert(S % 4 == 0, "FP32 records are whole float4s");
+    const float4* r4 = reinterpret_cast<const float4*>(rec + (size_t)i * S);
+#pragma unroll
+    for (int q = 0; q < S / 4; ++q) {
+        const float4 v = __ldg(r4 + q);
+        out[4 * q] = v.x;
+        out[4 * q + 1] = v.y;
+        out[4 * q + 2] = v.z;
+        out[4 * q + 3] = v.w;
+    }
+}
+
 // One work item of the FP32-compensated sweep (see f64_item).
 template <int D, int R, int V>
 __device__ __forceinline__ void f32c_item(const float* __restrict__ rec,
@@ -891,7 +908,8 @@ __device__ __forceinline__ void f32c_item(const float* __restrict__ rec,
     for (int r = 0; r < R; ++r) {
         const int iRaw = stripBase + r * kSweepThreads + tid;
         const int i = ordered ? rowOrder[iRaw] : min(iRaw, N - 1);
-        const float* ri = rec + (size_t)i * S;
+        float ri[S];
+        load_record_f32<S>(rec, i, ri);
 #pragma unroll
         for (int k = 0; k < D; ++k) {
             w.xh[r][k] = dup2(ri[k]);
@@ -932,7 +950,8 @@ __device__ __forceinline__ void f32c_item(const float* __restrict__ rec,
         __syncthreads();
         // stage the tile: one thread per column, fields negated
         if (tid < nj) {
-            const float* rj = rec + (size_t)(j0 + tid) * S;
+            float rj[S];
+            load_record_f32<S>(rec, j0 + tid, rj);
 #pragma unroll
             for (int k = 0; k < D; ++k) {
                 st.nx[k][tid] = -rj[k];
