@@ -1298,15 +1298,36 @@ int hphc_multiset_set_data(hphc_multiset* m, int set, const double* locations, s
                    "set %d: lengths %zu, %zu != D*N = %zu, N = %d", set, locLength, timesLength,
                    (size_t)es.N * m->D, es.N);
     size_t bad = 0;
-    if (!all_finite(locations, locLength, &bad) || !all_finite(times, timesLength, &bad))
-        return fmt(m->lastError, HPHC_ERR_NONFINITE, "set %d: non-finite input", set);
     DeviceGuard g(m->rt.device);
     if (!g.ok) return fmt(m->lastError, HPHC_ERR_CUDA, "cannot select device %d", m->rt.device);
-    cudaError_t e = cudaEventSynchronize(m->uploaded[set]);  // the last copy from the mirror
-    if (e != cudaSuccess) return cuda_status(m->lastError, e, "wait for the set's upload");
-    std::memcpy(m->hLoc[set].p, locations, locLength * sizeof(double));
-    std::memcpy(es.hTimes.p, times, timesLength * sizeof(double));
-    es.derive_times();
+    cudaError_t e;
+    int ascending = -1;
+    if (m->ready[set] && !m->dirty[set]) {
+        // The device holds the set's current data, so the new values are
+        // checked while they are copied into the mirrors (one pass each);
+        // a rejected input has the mirrors restored from the device copy.
+        if ((e = cudaEventSynchronize(m->uploaded[set])) != cudaSuccess)
+            return cuda_status(m->lastError, e, "wait for the set's upload");
+        bool asc = false;
+        if (!copy_checked<false>(locations, m->hLoc[set].p, locLength, &bad, nullptr) ||
+            !copy_checked<true>(times, es.hTimes.p, timesLength, &bad, &asc)) {
+            if ((e = cudaMemcpy(m->hLoc[set].p, es.dLoc.p, locLength * sizeof(double),
+                                cudaMemcpyDeviceToHost)) ||
+                (e = cudaMemcpy(es.hTimes.p, es.dTimes.p, timesLength * sizeof(double),
+                                cudaMemcpyDeviceToHost)))
+                return cuda_status(m->lastError, e, "restore the set after a rejected input");
+            return fmt(m->lastError, HPHC_ERR_NONFINITE, "set %d: non-finite input", set);
+        }
+        ascending = asc ? 1 : 0;
+    } else {
+        if (!all_finite(locations, locLength, &bad) || !all_finite(times, timesLength, &bad))
+            return fmt(m->lastError, HPHC_ERR_NONFINITE, "set %d: non-finite input", set);
+        if ((e = cudaEventSynchronize(m->uploaded[set])) != cudaSuccess)
+            return cuda_status(m->lastError, e, "wait for the set's upload");
+        std::memcpy(m->hLoc[set].p, locations, locLength * sizeof(double));
+        std::memcpy(es.hTimes.p, times, timesLength * sizeof(double));
+    }
+    es.derive_times(ascending);
     m->ready[set] = 1;
     m->dirty[set] = 1;
     // upload now, overlapping the host work on the next sets

@@ -104,7 +104,8 @@ def test_multiset_equals_single_engines():
             e.setParameters(p)
             l1, g1 = e.getLogLikelihoodAndGradient()
         # the same sums; the autotuner may pick another sweep shape for the
-        # multiset than for one set, which only reorders FP32 block sums
+        # multiset than for one set: other strips (which pairs are summed as
+        # the FP32 column sums of the symmetric sweep) and other j-chunks
         assert abs(l1 - ll[s]) <= 1e-9 * abs(l1)
         assert np.all(np.abs(g1 - g[s]) <= 1e-7 * (np.abs(g1) + 1.0))
 
@@ -142,6 +143,43 @@ def test_multiset_errors():
         with pytest.raises(hb.HawkesError) as ei:
             m.setData(2, np.zeros(400), np.zeros(200))
         assert ei.value.status == 3
+
+
+@pytest.mark.parametrize("flags", [FP64, FP32C], ids=["fp64", "fp32c"])
+def test_multiset_rejected_input_leaves_the_set_unchanged(flags):
+    # A set that holds data checks new values while copying them into its
+    # host mirror and restores the mirror from the device copy when one is
+    # not finite; a set without data checks before copying.  Either way the
+    # set keeps its previous events.
+    sets = workloads.uneven(3, seed=44, lo=300, hi=2000)
+    params = np.stack([p for _, _, p in sets])
+    with hb.Multiset(2, [len(t) for _, t, _ in sets], flags, 0) as m:
+        bad_loc = np.array(sets[0][0], dtype=np.float64)
+        bad_loc.reshape(-1)[7] = np.nan
+        with pytest.raises(hb.HawkesError) as ei:
+            m.setData(0, bad_loc, sets[0][1])
+        assert ei.value.status == 4  # non-finite, before the set had data
+        for s, (loc, t, _) in enumerate(sets):
+            m.setData(s, loc, t)
+        ll0, g0 = m.logLikelihoodAndGradient(params)
+        other_loc, other_t = workloads.uniform(len(sets[1][1]), seed=45)
+        bad_t = np.array(other_t)
+        bad_t[-3] = np.inf
+        with pytest.raises(hb.HawkesError) as ei:
+            m.setData(1, other_loc, bad_t)  # locations copied, then the times rejected
+        assert ei.value.status == 4
+        loc2, t2 = workloads.uniform(len(sets[2][1]), seed=46)
+        loc2 = np.array(loc2, dtype=np.float64)
+        loc2.reshape(-1)[-1] = np.nan
+        with pytest.raises(hb.HawkesError) as ei:
+            m.setData(2, loc2, t2)  # rejected in the locations
+        assert ei.value.status == 4
+        ll1, g1 = m.logLikelihoodAndGradient(params)
+        assert np.array_equal(ll0, ll1) and np.array_equal(g0, g1)
+        # accepted new data still replaces the set
+        m.setData(1, other_loc, other_t)
+        ll2, _ = m.logLikelihoodAndGradient(params)
+        assert ll2[1] != ll0[1] and ll2[0] == ll0[0] and ll2[2] == ll0[2]
 
 
 @pytest.mark.parametrize("flags", [FP64, FP32C], ids=["fp64", "fp32c"])
