@@ -67,7 +67,8 @@ L2_FLUSH_BYTES = 256 << 20
 # equivalent and can exceed the pipe's peak.
 FP32_PER_PAIR_EVAL, EX2_PER_PAIR_EVAL = 13.5, 1.5
 FP32_PER_B, FP32_PER_COL, FP32_PER_S = 11.0, 3.0, 5.0
-# The FP32-compensated algorithm adds to that count the work its precision
+# The roofline counts the algorithm, not its compensation.  As a second
+# figure, the FP32-compensated implementation adds the work its precision
 # pattern requires: every near background term (a tile pair not in the far
 # tail) and every self-excitation term takes its time difference from hi and
 # lo parts (+2) and enters its three sums by Fast2Sum (+3 each, +9); far-tail
@@ -561,12 +562,13 @@ def ours_arm(args):
     sweep_mean = statistics.mean(sweep32)
     # the roofline counts the terms the launch evaluated; "effective" counts
     # the brute-force work (every ordered pair) the launch stands for
-    inst_plain = FP32_PER_B * nev + FP32_PER_COL * (nb - nev) + FP32_PER_S * ns
+    # algorithmic count of the evaluated terms (compensation not counted)
+    inst = FP32_PER_B * nev + FP32_PER_COL * (nb - nev) + FP32_PER_S * ns
+    achieved = inst / (sweep_mean / 1e3) / 1e12
     far = (far_tail_share(w["t"], w["params"][2], shape32[0])
            if w["kind"] == "single" and shape32 else 1.0)
-    inst = (FP32C_PER_NEAR_B * (1.0 - far) * nev + FP32_PER_B * far * nev +
-            FP32_PER_COL * (nb - nev) + FP32C_PER_S * ns)
-    achieved = inst / (sweep_mean / 1e3) / 1e12
+    inst_comp = (FP32C_PER_NEAR_B * (1.0 - far) * nev + FP32_PER_B * far * nev +
+                 FP32_PER_COL * (nb - nev) + FP32C_PER_S * ns)
     ncu = None
     npath = os.path.join(ROOT, "profiles", "sweep_pipes.json")
     if os.path.exists(npath):
@@ -622,21 +624,22 @@ def ours_arm(args):
         "roofline": {"bound": "fp32", "kernel": kernel,
                      "achieved": achieved, "peak": peak_inst, "unit": "Tinst/s",
                      "frac": achieved / peak_inst, "traffic": traffic,
-                     "count": "FP32 instructions (FMA = 1) of the compensated algorithm on the "
-                              "terms this launch evaluated: "
-                              f"{FP32C_PER_NEAR_B:g} per near background exponential (hi/lo time "
-                              "difference, three Fast2Sum additions), "
-                              f"{FP32_PER_B:g} per far-tail one ({far:.3f} of them), "
-                              f"{FP32_PER_COL:g} per background pair also added to the earlier "
-                              f"event's sums, {FP32C_PER_S:g} per self-excitation term; over the "
-                              "mean CUDA-event duration of the sweep kernel",
+                     "count": "FP32 instructions (FMA = 1) of the terms this launch evaluated, "
+                              "compensation not counted: "
+                              f"{FP32_PER_B:g} per background exponential, {FP32_PER_COL:g} per "
+                              "background pair also added to the earlier event's sums, "
+                              f"{FP32_PER_S:g} per self-excitation term; over the mean "
+                              "CUDA-event duration of the sweep kernel",
                      "instructions_per_launch": inst,
-                     "plain_count": {"instructions_per_launch": inst_plain,
-                                     "frac": inst_plain / (sweep_mean / 1e3) / 1e12 / peak_inst,
-                                     "count": f"without the compensation: {FP32_PER_B:g} per "
-                                              f"background exponential, {FP32_PER_S:g} per "
-                                              "self-excitation term"},
-                     "far_tail_share": far,
+                     "compensated_count": {
+                         "instructions_per_launch": inst_comp,
+                         "frac": inst_comp / (sweep_mean / 1e3) / 1e12 / peak_inst,
+                         "far_tail_share": far,
+                         "count": "the same terms with the work the precision pattern adds: "
+                                  f"{FP32C_PER_NEAR_B:g} per near background exponential (hi/lo "
+                                  "time difference, three Fast2Sum additions), "
+                                  f"{FP32_PER_B:g} per far-tail one, {FP32C_PER_S:g} per "
+                                  "self-excitation term"},
                      "ncu": ncu,
                      "peak_source": f"{sm_count} SMs x 128 FP32 lanes x {max_mhz:.0f} MHz "
                                     f"(sm_max_mhz, {peak_src})",
