@@ -450,10 +450,10 @@ sweep_f64_list_kernel(const SweepProblem* __restrict__ problems,
 // when the variant keeps their lo parts.  The self-excitation exponent
 // kS |dx'|^2 + kW dt' uses hi + lo coefficients so their FP32 rounding does
 // not bias every term in the same direction.  The weighted sums come out in
-// scaled units and the finish rescales them in FP64.  The six sums are kept in FP32 over
-// kFlush consecutive j and then added to FP64 accumulators (blocked
-// compensated summation); the cross-tile, cross-chunk and per-event finish are
-// FP64.
+// scaled units and the finish rescales them in FP64.  Each of a row's six sums
+// is a compensated FP32 pair (hi, lo; see RowSums below) over a work item's
+// whole j range, formed into FP64 when the item writes its partial sums; the
+// cross-chunk sums and the per-event finish are FP64.
 //
 // Variant bits (template parameter V):
 //   kSpaceLo  coordinate differences use the lo parts too (else hi only: the
