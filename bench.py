@@ -72,7 +72,7 @@ FP32_PER_B, FP32_PER_COL, FP32_PER_S = 11.0, 3.0, 5.0
 # pattern requires: every near background term (a tile pair not in the far
 # tail) and every self-excitation term takes its time difference from hi and
 # lo parts (+2) and enters its three sums by Fast2Sum (+3 each, +9); far-tail
-# background terms (each at most 2^-12 of the event's own term) and the
+# background terms (each at most 2^-10 of the event's own term) and the
 # symmetric column adds keep the plain count.
 FP32C_PER_NEAR_B, FP32C_PER_S = FP32_PER_B + 11.0, FP32_PER_S + 11.0
 FP32_LANES_PER_SM = 128
@@ -440,7 +440,7 @@ def far_tail_share(t, tau_t, R, tile=128, threads=128):
     in far-tail tile pairs, from the tile-pair decisions on sorted times:
     a strip of R tiles meets every tile up to its own last one; a pair is
     skipped when every background term is below 2^-60 (tail truncation), far
-    when below 2^-12 (log2 exponent -(b dt)^2 log2(e) / 2 over min |dt|)."""
+    when below 2^-10 (log2 exponent -(b dt)^2 log2(e) / 2 over min |dt|)."""
     t = np.asarray(t, dtype=np.float64)
     n = len(t)
     nt = (n + tile - 1) // tile
@@ -459,8 +459,8 @@ def far_tail_share(t, tau_t, R, tile=128, threads=128):
         e2 = k * gap * gap
         w = rows * cnt[j]
         keep = e2 < 60.0
-        far += float(np.sum(w[keep & (e2 >= 12.0)]))
-        near += float(np.sum(w[keep & (e2 < 12.0)]))
+        far += float(np.sum(w[keep & (e2 >= 10.0)]))
+        near += float(np.sum(w[keep & (e2 < 10.0)]))
     return far / max(near + far, 1.0)
 
 

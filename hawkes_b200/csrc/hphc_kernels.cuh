@@ -50,7 +50,7 @@ struct PairConsts {
     double skipB, skipS;                   // natural-log thresholds; < 0 disables
     // A tile pair whose background terms are all below exp(-fastB) (natural
     // log; <= 0 disables) takes them from the hardware ex2.approx: instead of
-    // the polynomial in the FP32 mode (2^-12, kFastTailLog2), of CUDA's exp()
+    // the polynomial in the FP32 mode (2^-10, kFastTailLog2), of CUDA's exp()
     // in the FP64 mode (2^-60, kFastTailLog2F64).
     double fastB;
     // Self-excitation-only sweep: no background term is evaluated (the
@@ -106,11 +106,15 @@ struct ConstsSpec {
 // Far background tail of the FP32 software-exponential mode.  A tile pair
 // whose background terms are all at most 2^-kFastTailLog2 of an event's own
 // term (B_ii = 1 unit) evaluates them with ex2.approx instead of the
-// polynomial.  Such terms lie beyond 3.46 scale units of the time Gaussian
-// (4.1 of its standard deviations), so they carry under 5e-4 of any
-// event's unit sums even weighted by dt'^2, and the hardware exponential's
-// relative error (< 1e-7) moves those sums by under ~5e-11.
-constexpr double kFastTailLog2 = 12.0;
+// polynomial.  Such terms lie beyond 3.16 scale units of the time Gaussian
+// (3.8 of its standard deviations).  At the headline density they carry
+// about 1.7e-4 of an event's background sum and 2.8e-3 of its sum weighted
+// by dt'^2 (4e-3 at most over 400 sampled events), so the hardware
+// exponential's relative error (< 1e-7, its mean divided out) moves those
+// sums by ~1e-10.  Measured at N = 100k against the oracle: 2^-10 is 2.4 %
+// faster than 2^-12 with the d/d tauT error 3.8e-9 -> 2.8e-9 (and lower at
+// N = 20k and 40k); 2^-8 is 5.7 % faster but puts d/d tauT at 2.8e-8.
+constexpr double kFastTailLog2 = 10.0;
 
 // FP64 mode: a tile pair whose background terms are all at most 2^-60 takes
 // them from the FP32 hardware exponential (relative error ~1e-7; zero below

@@ -465,8 +465,8 @@ sweep_f64_list_kernel(const SweepProblem* __restrict__ problems,
 //   kTimeHiOnly  background terms from the hi parts of the times only (far-tail
 //             tile pairs, set by the sweep itself): the lo parts are at most
 //             half an FP32 ulp of t' (~1e-6 in record units over the 8760 h
-//             span at the base tauT), which moves a far-tail term (|dt'| >= 3.46,
-//             at most 2^-12) by ~2.6e-6 |dt'| relative, with a sign that varies
+//             span at the base tauT), which moves a far-tail term (|dt'| >= 3.16,
+//             at most 2^-10) by ~2.6e-6 |dt'| relative, with a sign that varies
 //             with the pair.  Self-excitation terms of such a tile pair still
 //             use the full hi + lo difference.
 //   kPlain    FP32 throughout, the reference's single precision
@@ -537,7 +537,7 @@ __device__ __forceinline__ float2 exp2_poly_neg2(float2 s) {
 
 // Background unit terms 2^-(d2 + t2).  In the hardware-exponential variant its
 // mean relative error is divided out of the sums in the FP64 finish; far-tail
-// terms of the polynomial variant (at most 2^-12 each) keep it.
+// terms of the polynomial variant (at most 2^-10 each) keep it.
 template <int V>
 __device__ __forceinline__ float2 background2(float2 s) {
     if (V & kPolyExp) return exp2_poly_neg2(s);
@@ -633,7 +633,7 @@ __device__ __forceinline__ float2 self_dt2(const StagedTile<D>& t, int p, const 
 // The row value (hi - offset) + lo is formed in FP64 when the work item
 // writes its partial sums (hi - offset is exact there: two FP32 values).
 //
-// Far-tail background terms (each at most 2^-12 of the event's own term, see
+// Far-tail background terms (each at most 2^-10 of the event's own term, see
 // kFastTailLog2) are added to lo directly: lo then carries them and the
 // errors, both far below hi, and its own FP32 rounding is below 2^-24 of
 // that.

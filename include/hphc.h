@@ -82,7 +82,7 @@ extern "C" {
                                                 updates the kept per-event sums in O(N)) */
 #define HPHC_FLAG_NO_FAST_TAIL (1L << 15)    /* one exponential for every pair term (by
                                                 default tile pairs whose background terms are
-                                                all below 2^-12 (FP32-compensated mode) or
+                                                all below 2^-10 (FP32-compensated mode) or
                                                 2^-60 (FP64 mode) of an event's own term take
                                                 those terms from ex2.approx) */
 #define HPHC_FLAG_NO_TAIL_TRUNCATION (1L << 16) /* skip background tile pairs only where

@@ -4,13 +4,16 @@ proposals) and many event sets of uneven size, each evaluated in one run.
 Bars as in test_parity_gpu.py: FP64 plain 1e-10 relative on the
 log-likelihood and 1e-10 of the gradient's per-event scale; FP32-compensated
 1e-7 / 5e-6 of the term-level scale at small sizes.  A batched result and the
-same problem evaluated alone are split into different j-chunks.  In FP64 that
-changes only the order the chunk sums are added (1e-12 relative).  In the
+same problem evaluated alone are split into different j-chunks, and the
+autotuner may give them different strip heights.  In FP64 that changes only
+the order the chunk sums are added (1e-12 relative).  In the
 FP32-compensated mode each chunk's compensated FP32 sums start again, with
 exact errors, so the chunk bounds move the sums by the rounding of their
-error parts alone: measured under 1e-15 relative on the log-likelihood and
-3e-11 on the gradient (its d/d tauT component cancels ~400-fold); bars 1e-13
-and 2e-10.
+error parts alone, and another strip height moves which pairs go to the
+FP32 column sums: measured under 1e-15 relative on the log-likelihood and
+under 1e-12 of the gradient's per-event scale (2e-10 of |g| on the d/d tauT
+component, which cancels ~300-fold); bars 1e-13 and 1e-11 of the per-event
+scale.
 """
 import numpy as np
 import pytest
@@ -55,8 +58,9 @@ def test_proposals_match_single_evaluations_and_oracle(flags):
                 assert abs(lk - ll[k]) <= 1e-12 * abs(lk)
                 assert np.all(np.abs(gk - g[k]) <= 1e-12 * (np.abs(gk) + 1.0))
             else:
+                scale = oracle.oracle_eval(loc, t, P[k], threads=16)["grad_scale"]
                 assert abs(lk - ll[k]) <= 1e-13 * abs(lk)
-                assert np.all(np.abs(gk - g[k]) <= 2e-10 * (np.abs(gk) + 1.0))
+                assert np.all(np.abs(gk - g[k]) <= 1e-11 * scale)
     for k in (3, 29):
         o = oracle.oracle_eval(loc, t, P[k], threads=16)
         check_vs_oracle(ll[k], g[k], o, flags, f"proposal {k}")
