@@ -435,7 +435,7 @@ def make_workload(name, n):
     raise ValueError(name)
 
 
-def far_tail_share(t, tau_t, R, tile=128, threads=128):
+def far_tail_share(t, tau_t, R, tile=128):
     """Share of the symmetric FP32 sweep's background exponentials that fall
     in far-tail tile pairs, from the tile-pair decisions on sorted times:
     a strip of R tiles meets every tile up to its own last one; a pair is

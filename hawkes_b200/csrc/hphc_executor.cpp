@@ -98,12 +98,15 @@ void strip_band(const SetView& s, const PairConsts& c, bool symmetric, bool wide
 // the background terms take the full exponential ("near"), beyond it the
 // far tail's cheaper one; below dS the tile also holds self-excitation
 // terms.  Weights from measured sweep times: a far-tail tile costs about
-// 3/4 of a near one in the FP32 mode and 7/10 in the FP64 mode; the
-// self-excitation terms of a tile add about half a tile in the FP32 mode
-// and a whole one in the FP64 mode (CUDA's exp() for each).  Ordering by
-// these costs instead of tile counts: sweep at N = 100k 2.588 -> 2.498 ms
-// (FP32) and 10.06 -> 9.69 ms (FP64).
-constexpr double kFarTileCostF32 = 0.75;
+// half a near one in the FP32-compensated mode (whose near terms take the
+// software exponential and three compensated sums) and 7/10 in the FP64
+// mode; the self-excitation terms of a tile add about half a tile in the
+// FP32 mode and a whole one in the FP64 mode (CUDA's exp() for each).
+// Ordering by these costs instead of tile counts: sweep at N = 100k 2.588 ->
+// 2.498 ms (FP32, plain block sums then) and 10.06 -> 9.69 ms (FP64); the
+// FP32 far weight 0.75 -> 0.5 with the compensated sums: 2.676 -> 2.620 ms
+// at 64 items/SM, 2.81 -> 2.64 ms at 32.
+constexpr double kFarTileCostF32 = 0.5;
 constexpr double kFarTileCostF64 = 0.70;
 constexpr double kSelfTileCostF32 = 0.5;
 constexpr double kSelfTileCostF64 = 1.0;
