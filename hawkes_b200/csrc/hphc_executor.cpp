@@ -169,6 +169,7 @@ std::map<TuneKey, std::pair<int, int>> gTuneCache;
 // line is written with one append of under 200 bytes, so processes sharing
 // the file do not interleave their lines.
 constexpr int kTuneCacheVersion = 1;
+constexpr int kTuneReps = 4;  // timed sweeps per candidate shape (even)
 
 struct TuneLine {
     std::string device;
@@ -791,9 +792,12 @@ int Executor::autotune(const std::vector<SetView>& sets, const int* setOf, const
             itemsPerSM = it;
             if ((st = build_plan(sets, setOf, params, P, dProbs, r, it))) break;
             const int grid = sweep_grid(r);
-            // best of three sweeps (the first also warms the caches)
-            float ms = 1e30f;
-            for (int rep = 0; rep < 3 && !st; ++rep) {
+            // median of four sweeps after one that warms the caches: the
+            // shapes' typical times differ by ~1 %, about as much as the
+            // best of a few launches varies
+            float times[kTuneReps];
+            int nt = 0;
+            for (int rep = 0; rep <= kTuneReps && !st; ++rep) {
                 if ((st = launch_sequence(grid))) break;
                 cudaError_t e = cudaStreamSynchronize(stream_);
                 float t = 0.f;
@@ -802,7 +806,12 @@ int Executor::autotune(const std::vector<SetView>& sets, const int* setOf, const
                     st = cuda_fail(e, "autotune timing");
                     break;
                 }
-                ms = std::min(ms, t);
+                if (rep > 0) times[nt++] = t;
+            }
+            float ms = 1e30f;
+            if (!st && nt == kTuneReps) {
+                std::sort(times, times + nt);
+                ms = 0.5f * (times[nt / 2 - 1] + times[nt / 2]);
             }
             if (st) break;
             if (ms < best) {
