@@ -214,6 +214,42 @@ def test_repeatable_bits(flags):
     assert r1[0] == r2[0] and np.array_equal(r1[1], r2[1])
 
 
+@pytest.mark.parametrize("flags", [FP64, FP32C], ids=["fp64", "fp32c"])
+def test_sweep_shapes_agree(flags):
+    # The FP64 sums and the FP32-compensated row sums (exact errors from a
+    # power-of-two start) do not depend on the j-chunks, so shapes with the
+    # same events per thread R agree to rounding.  In the FP32 mode another R
+    # makes other strips: the tile-pair decisions (software or far-tail
+    # exponential, the truncated tail) and the pairs left to the symmetric
+    # sweep's FP32 column sums change, so those results differ within the
+    # mode's own error against the oracle (measured R = 2 against R = 4:
+    # 3.3e-11 on the log-likelihood, 3.0e-9 of the per-event scale on the
+    # gradient, mostly from the far-tail tile pairs that the wider strips
+    # classify as near; bars 2e-10 and half the mode's 1e-8).
+    loc, t = workloads.uniform(20000, seed=13)
+    p = workloads.BASE_PARAMS
+    scale = oracle.oracle_eval(loc, t, p, threads=16)["grad_scale"]
+    shapes = [(1, 8), (1, 64), (2, 8), (2, 64)] if flags == FP64 else \
+        [(2, 8), (2, 64), (4, 8), (4, 64)]
+    out = {}
+    with engine(loc, t, p, flags | hb.NO_INCREMENTAL) as e:
+        for shape in shapes:
+            e.setSweepShape(*shape)
+            ll, g = e.getLogLikelihoodAndGradient()
+            out[shape] = (ll, np.asarray(g))
+    ll0, g0 = out[shapes[0]]
+    for shape, (ll, g) in out.items():
+        same_r = shape[0] == shapes[0][0]
+        if flags == FP64:
+            assert abs(ll - ll0) <= 1e-13 * abs(ll0), shape
+            assert np.all(np.abs(g - g0) <= 1e-12 * scale), shape
+        else:
+            print(shape, f"loglik {abs(ll - ll0) / abs(ll0):.2e}",
+                  f"grad/event-scale {np.max(np.abs(g - g0) / scale):.2e}")
+            assert abs(ll - ll0) <= (1e-13 if same_r else 2e-10) * abs(ll0), shape
+            assert np.all(np.abs(g - g0) <= (1e-12 if same_r else 5e-9) * scale), shape
+
+
 def test_single_row_updates_equal_full_update():
     loc, t = workloads.uniform(777, seed=9)
     p = workloads.BASE_PARAMS
