@@ -55,3 +55,43 @@ def test_single_rank_needs_no_process_group():
 def test_whole_job_rate():
     # 2 ranks x 1e10 pair-evals each over the slowest rank's 5 ms
     assert bench.whole_job_rate(2, 1e10, 5.0) == pytest.approx(4e12)
+
+
+_REF_ARM = r"""
+import json, runpy, sys
+sys.argv = ["bench.py", "--impl", "reference", "--steps", "1", "--warmup", "1", "--n", "2000"]
+try:
+    runpy.run_path("bench.py", run_name="__main__")
+except SystemExit:
+    pass
+maps = open("/proc/self/maps").read()
+libs = sorted({l.split()[-1] for l in maps.splitlines() if l.split()[-1].endswith(".so")
+               and ("/oracle/" in l or "/hawkes_b200/" in l)})
+print("MAPPED " + json.dumps(libs))
+"""
+
+
+def test_reference_arm_line_and_libraries():
+    # The reference arm prints one JSON line with the contract's keys and maps
+    # the reference engine's library only, never the CUDA engine's.
+    import json
+    import subprocess
+    import sys
+
+    import oracle
+    if not oracle.ref_available():
+        pytest.skip("reference engine (oracle/_ref) not built")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", _REF_ARM], cwd=root, capture_output=True,
+                       text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    line = json.loads(lines[-1])
+    for key in ("impl", "metric", "value", "unit", "n_gpus", "steps", "warmup",
+                "ms_per_step", "higher_is_better", "config", "cpu_baseline", "e2e"):
+        assert key in line, key
+    assert line["impl"] == "reference" and line["value"] > 0
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["cpu_baseline"]["kind"] == "reference"
+    mapped = json.loads([l for l in r.stdout.splitlines() if l.startswith("MAPPED ")][-1][7:])
+    assert any(m.endswith("oracle/_ref/libhawkes_ref.so") for m in mapped), mapped
+    assert not any("libhawkes_b200" in m for m in mapped), mapped
