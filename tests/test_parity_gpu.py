@@ -105,6 +105,27 @@ def test_random_cases_against_oracle(flags):
 
 
 @pytest.mark.parametrize("flags", MODES, ids=IDS)
+def test_wide_kernels_against_oracle(flags):
+    # Self-excitation kernels wider than the background's: a small sigma
+    # (wide in space) and a small omega (slow decay) make single terms of the
+    # sums S d'^2 and S dt' exceed 1 in record units, so the compensated row
+    # sums start from a larger power-of-two offset there (here 8 and 2 for
+    # S d'^2 in the first two cases, 2 for S dt' in the last).
+    rng = np.random.default_rng(91)
+    for N, D, scale in ((1200, 2, (0.2, 1.0, 1.0, 0.05, 1.0, 1.0)),
+                        (900, 3, (0.35, 1.0, 2.0, 0.2, 0.5, 2.0)),
+                        (800, 2, (0.5, 1.0, 1.0, 5e-4, 1.0, 1.0))):
+        loc = rng.uniform(0, 12, size=(N, D))
+        t = np.sort(rng.uniform(0, 2000, size=N))
+        p = workloads.BASE_PARAMS * np.array(scale)
+        o = oracle.oracle_eval(loc, t, p, threads=8)
+        c = {"loc": loc, "t": t, "params": p, "ref_loglik": o["loglik"],
+             "ref_probs": o["probs"], "oracle_grad": o["grad"], "grad_scale": o["grad_scale"],
+             "grad_term_scale": o["grad_term_scale"]}
+        check_case(f"wide_D{D}_N{N}", c, flags)
+
+
+@pytest.mark.parametrize("flags", MODES, ids=IDS)
 def test_unsorted_times_against_oracle(flags):
     # Times in no particular order (the last one is the largest, so T bounds
     # them): every tile pair may hold self-excitation terms in either order.
