@@ -104,6 +104,34 @@ def test_random_cases_against_oracle(flags):
         check_case(f"trial{trial}_D{D}_N{N}", c, flags)
 
 
+@pytest.mark.parametrize("flags", [FP64, FP32C], ids=["fp64", "fp32c"])
+def test_block_boundary_sizes_against_oracle(flags):
+    # Event counts at tile (128) and strip (256 events at R = 2, 512 at R = 4)
+    # boundaries, with tie-heavy times: the last partial tile and strip, the
+    # padding rows and columns, and (FP32 modes) the spatial row order of the
+    # full strips, at both strip heights.
+    rng = np.random.default_rng(131)
+    shapes = [(1, 16), (2, 16)] if flags == FP64 else [(2, 16), (4, 16)]
+    for N in (1, 2, 127, 128, 129, 255, 256, 257, 511, 512, 513):
+        loc = rng.uniform(0, 6, size=(N, 2))
+        t = np.sort(np.round(rng.uniform(0, 400, size=N), 0))  # many exact ties
+        p = workloads.BASE_PARAMS * np.array([1.0, 1.0, 4.0, 1.0, 1.0, 1.0])
+        o = oracle.oracle_eval(loc, t, p, threads=8)
+        tol = TOL[flags]
+        key = "grad_scale" if flags == FP64 else "grad_term_scale"
+        allowed = tol["grad"] * np.maximum(o[key], 1e-300) + \
+            (0.0 if flags == FP64 else 1e-12 * np.max(o[key]))
+        for shape in shapes:
+            with engine(loc, t, p, flags) as e:
+                e.setSweepShape(*shape)
+                ll, g = e.getLogLikelihoodAndGradient()
+                probs = e.getProbsSelfExcite()
+            tag = (N, shape)
+            assert abs(ll - o["loglik"]) <= tol["ll"] * abs(o["loglik"]), tag
+            assert np.all(np.abs(np.asarray(g) - o["grad"]) <= allowed), tag
+            assert np.max(np.abs(probs - o["probs"])) <= tol["probs"], tag
+
+
 @pytest.mark.parametrize("flags", MODES, ids=IDS)
 def test_wide_kernels_against_oracle(flags):
     # Self-excitation kernels wider than the background's: a small sigma
